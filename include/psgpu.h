@@ -1,0 +1,135 @@
+/*
+ * psgpu.h -- the C ABI of the B200 prime / k-tuplet counting engine.
+ *
+ * This is the thin boundary the host layers (the primesieve-compatible C and
+ * C++ APIs, the CLI, and foreign-language bindings) call. Plain C types only:
+ * integers, pointers, sizes and an opaque context handle. Every function
+ * returns a psg_status; on failure a message is available from
+ * psg_last_error() (thread-local). Nothing here throws.
+ *
+ * Reference interfaces each entry point replaces (paths inside the reference
+ * project):
+ *   psg_count            GpuBackend::count(lo, hi, countType)
+ *                        src/gpu/GpuBackend.hpp:66-69 and countOnGpu()
+ *                        src/gpu/GpuSieve.cpp:131-176 (incl. the 2/3/5 table),
+ *                        widened to all six counts in one pass.
+ *   psg_count_batch      no counterpart (the reference counts one range per
+ *                        call: src/api.cpp:48-118).
+ *   psg_init / psg_destroy  CudaBackend::init / ~CudaBackend
+ *                        src/gpu/cuda/CudaBackend.cpp:222-344, :114-123.
+ *   psg_device_count / psg_device_describe  listDevices(), DeviceInfo::describe()
+ *                        src/gpu/GpuSieve.cpp:43-72.
+ *   psg_config fields    GpuConfig src/gpu/GpuBackend.hpp:45-58 and the
+ *                        set_gpu_* knobs include/primesieve/gpu.hpp:48-53.
+ */
+#ifndef PSGPU_H
+#define PSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PSG_OK = 0,
+  PSG_ERR_ARG = 1,        /* invalid argument (e.g. start > stop where not allowed) */
+  PSG_ERR_NO_DEVICE = 2,  /* no usable CUDA device / bad device index */
+  PSG_ERR_CUDA = 3,       /* a CUDA runtime call failed */
+  PSG_ERR_NOMEM = 4,      /* device or host allocation failed */
+  PSG_ERR_LIMIT = 5,      /* request beyond a documented maximum */
+  PSG_ERR_INTERNAL = 6,   /* internal consistency check failed */
+  PSG_ERR_TIMEOUT = 7,    /* a bounded wait gave up */
+  PSG_ERR_CLOSED = 8      /* the server / queue has been shut down */
+} psg_status;
+
+/* Count kinds: bit i of a kinds mask selects counts[i]. */
+enum {
+  PSG_PRIMES = 1u << 0,
+  PSG_TWINS = 1u << 1,
+  PSG_TRIPLETS = 1u << 2,
+  PSG_QUADRUPLETS = 1u << 3,
+  PSG_QUINTUPLETS = 1u << 4,
+  PSG_SEXTUPLETS = 1u << 5,
+  PSG_ALL_KINDS = 0x3fu
+};
+
+typedef struct psg_context psg_context;
+
+/* Tuning knobs; 0 means "auto". Mirrors GpuConfig plus the big-prime and
+ * batching parameters this engine adds. */
+typedef struct {
+  uint32_t seg_bytes;          /* shared-memory sieve segment per CTA (bytes) */
+  uint32_t block;              /* threads per CTA: 256, 512 or 1024 */
+  uint32_t ctas_per_sm;        /* resident sieve CTAs per SM */
+  uint32_t small_limit;        /* sieving primes below: one warp per prime */
+  uint32_t big_limit;          /* sieving primes from: bucket sieve */
+  uint32_t window_segments;    /* segments per bucket window */
+  uint32_t bucket_lists;       /* bucket lists per segment */
+  uint32_t presieve;           /* 1 = pre-sieve with pattern tables (default) */
+  uint32_t segments_per_launch;/* cap on segments per launch (reference knob) */
+} psg_config;
+
+/* A [start, stop] range and the kinds wanted for it (batch API). */
+typedef struct {
+  uint64_t start;
+  uint64_t stop;
+  uint32_t kinds;
+  uint32_t reserved;
+} psg_range;
+
+/* ---- devices ------------------------------------------------------------ */
+int psg_device_count(int* count);
+/* One human-readable line for device `index`. */
+int psg_device_describe(int index, char* buf, size_t len);
+
+/* ---- context ------------------------------------------------------------ */
+/* device < 0 picks the device with the most SMs. cfg may be NULL. */
+int psg_init(int device, const psg_config* cfg, psg_context** out);
+void psg_destroy(psg_context* ctx);
+/* The configuration actually in use (autotuned values filled in). */
+int psg_get_config(const psg_context* ctx, psg_config* out);
+int psg_describe(const psg_context* ctx, char* buf, size_t len);
+
+/* ---- counting ----------------------------------------------------------- */
+/* Count primes and/or k-tuplets in [start, stop] (0 <= start, stop <= 2^64-1).
+ * counts[i] receives the count of kind i if bit i of kinds is set, else 0.
+ * start > stop gives all zeros. Synchronous. */
+int psg_count(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
+              uint64_t counts[6]);
+
+/* Asynchronous variant: ADDS the counts to dev_counts (device memory,
+ * 6 x uint64_t) on `stream` (a cudaStream_t, NULL = the context's stream).
+ * The 2/3/5 table is included. Host-side preparation (the sieving-prime
+ * table for sqrt(stop)) happens before return. */
+int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
+                    uint64_t* dev_counts, void* stream);
+
+/* Count n ranges; counts is n x 6 (row i for ranges[i]). */
+int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n,
+                    uint64_t* counts);
+
+/* Build the sieving-prime table up to sqrt(stop) ahead of time. */
+int psg_prepare(psg_context* ctx, uint64_t stop);
+
+/* ---- diagnostics -------------------------------------------------------- */
+const char* psg_last_error(void);
+const char* psg_status_string(int status);
+
+/* Per-kernel CUDA-event timing of this context's launches. */
+int psg_set_profiling(psg_context* ctx, int on);
+/* Fills up to `cap` entries: name (static string), launches, total ms.
+ * *n receives the number of kernels. */
+int psg_kernel_stats(psg_context* ctx, const char** names, uint64_t* launches,
+                     double* ms, size_t cap, size_t* n);
+int psg_reset_kernel_stats(psg_context* ctx);
+
+/* The library version string. */
+const char* psg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

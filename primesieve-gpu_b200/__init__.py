@@ -1,0 +1,204 @@
+"""Python binding of the B200 prime / k-tuplet counting engine (ctypes).
+
+The engine itself is C++/CUDA in ``lib/libprimesieve_gpu.so``; this module
+only loads it and mirrors its C ABI (``include/psgpu.h``) and the
+primesieve-compatible count API (``include/primesieve.h``). There is no
+Python or CPU fallback: if the shared library or a CUDA device is missing,
+every counting call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libprimesieve_gpu.so")
+CLI_PATH = os.path.join(HERE, "bin", "primesieve")
+
+PRIMES, TWINS, TRIPLETS, QUADRUPLETS, QUINTUPLETS, SEXTUPLETS = (1 << i for i in range(6))
+ALL_KINDS = 0x3F
+KIND_NAMES = ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets")
+PRIMESIEVE_ERROR = (1 << 64) - 1
+
+# Exported symbols of the C ABI and of the primesieve-compatible C API.
+PSG_SYMBOLS = (
+    "psg_device_count", "psg_device_describe", "psg_init", "psg_destroy",
+    "psg_get_config", "psg_describe", "psg_count", "psg_count_async",
+    "psg_count_batch", "psg_prepare", "psg_last_error", "psg_status_string",
+    "psg_set_profiling", "psg_kernel_stats", "psg_reset_kernel_stats", "psg_version",
+)
+
+
+class PsgError(RuntimeError):
+    """A psg_* call returned a non-zero status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"psg status {status}: {message}")
+        self.status = status
+
+
+class PsgConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in (
+        "seg_bytes", "block", "ctas_per_sm", "small_limit", "big_limit",
+        "window_segments", "bucket_lists", "presieve", "segments_per_launch")]
+
+
+class PsgRange(ctypes.Structure):
+    _fields_ = [("start", ctypes.c_uint64), ("stop", ctypes.c_uint64),
+                ("kinds", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the engine library and declare the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with `make -C primesieve-gpu_b200`")
+    lib = ctypes.CDLL(path)
+    u64, u32, i32, vp, sz = (ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int,
+                             ctypes.c_void_p, ctypes.c_size_t)
+    U64P = ctypes.POINTER(ctypes.c_uint64)
+    lib.psg_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    lib.psg_device_describe.argtypes = [i32, ctypes.c_char_p, sz]
+    lib.psg_init.argtypes = [i32, ctypes.POINTER(PsgConfig), ctypes.POINTER(vp)]
+    lib.psg_destroy.argtypes = [vp]
+    lib.psg_destroy.restype = None
+    lib.psg_get_config.argtypes = [vp, ctypes.POINTER(PsgConfig)]
+    lib.psg_describe.argtypes = [vp, ctypes.c_char_p, sz]
+    lib.psg_count.argtypes = [vp, u64, u64, u32, U64P]
+    lib.psg_count_async.argtypes = [vp, u64, u64, u32, vp, vp]
+    lib.psg_count_batch.argtypes = [vp, ctypes.POINTER(PsgRange), sz, U64P]
+    lib.psg_prepare.argtypes = [vp, u64]
+    lib.psg_last_error.restype = ctypes.c_char_p
+    lib.psg_status_string.restype = ctypes.c_char_p
+    lib.psg_status_string.argtypes = [i32]
+    lib.psg_set_profiling.argtypes = [vp, i32]
+    lib.psg_kernel_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), U64P,
+                                     ctypes.POINTER(ctypes.c_double), sz, ctypes.POINTER(sz)]
+    lib.psg_reset_kernel_stats.argtypes = [vp]
+    lib.psg_version.restype = ctypes.c_char_p
+    for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
+        fn = getattr(lib, "primesieve_count_" + name, None)
+        if fn is not None:
+            fn.argtypes = [u64, u64]
+            fn.restype = u64
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        lib = load()
+        raise PsgError(status, (lib.psg_last_error() or b"").decode(errors="replace"))
+
+
+def device_count() -> int:
+    n = ctypes.c_int(0)
+    _check(load().psg_device_count(ctypes.byref(n)))
+    return n.value
+
+
+class Context:
+    """One engine context on one CUDA device (``psg_init``)."""
+
+    def __init__(self, device: int = -1, **config: int):
+        lib = load()
+        cfg = PsgConfig()
+        for k, v in config.items():
+            setattr(cfg, k, int(v))
+        h = ctypes.c_void_p()
+        _check(lib.psg_init(device, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.psg_destroy(self._h)
+            self._h = None
+
+    def __enter__(self) -> "Context":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def config(self) -> dict:
+        c = PsgConfig()
+        _check(self._lib.psg_get_config(self._h, ctypes.byref(c)))
+        return {n: getattr(c, n) for n, _ in PsgConfig._fields_}
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _check(self._lib.psg_describe(self._h, buf, 512))
+        return buf.value.decode()
+
+    def count(self, start: int, stop: int, kinds: int = ALL_KINDS) -> List[int]:
+        out = (ctypes.c_uint64 * 6)()
+        _check(self._lib.psg_count(self._h, start, stop, kinds, out))
+        return list(out)
+
+    def count_async(self, start: int, stop: int, kinds: int, dev_counts_ptr: int,
+                    stream_ptr: int = 0) -> None:
+        _check(self._lib.psg_count_async(self._h, start, stop, kinds,
+                                         ctypes.c_void_p(dev_counts_ptr),
+                                         ctypes.c_void_p(stream_ptr or None)))
+
+    def count_batch(self, ranges: Sequence[Tuple[int, int, int]]) -> List[List[int]]:
+        n = len(ranges)
+        arr = (PsgRange * max(n, 1))()
+        for i, (a, b, k) in enumerate(ranges):
+            arr[i].start, arr[i].stop, arr[i].kinds = a, b, k
+        out = (ctypes.c_uint64 * (6 * max(n, 1)))()
+        _check(self._lib.psg_count_batch(self._h, arr, n, out))
+        return [list(out[6 * i:6 * i + 6]) for i in range(n)]
+
+    def prepare(self, stop: int) -> None:
+        _check(self._lib.psg_prepare(self._h, stop))
+
+    def set_profiling(self, on: bool) -> None:
+        _check(self._lib.psg_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_stats(self) -> dict:
+        cap = 16
+        names = (ctypes.c_char_p * cap)()
+        launches = (ctypes.c_uint64 * cap)()
+        ms = (ctypes.c_double * cap)()
+        n = ctypes.c_size_t(0)
+        _check(self._lib.psg_kernel_stats(self._h, names, launches, ms, cap, ctypes.byref(n)))
+        return {names[i].decode(): (launches[i], ms[i]) for i in range(min(n.value, cap))}
+
+    def reset_kernel_stats(self) -> None:
+        _check(self._lib.psg_reset_kernel_stats(self._h))
+
+
+def split_range(start: int, stop: int, parts: int) -> List[Tuple[int, int]]:
+    """Split [start, stop] into `parts` consecutive sub-ranges whose inner
+    boundaries are == 2 (mod 30), so that no k-tuplet straddles two parts
+    (reference src/ParallelSieve.cpp:122-133). Empty parts are dropped."""
+    if start > stop:
+        return []
+    parts = max(1, parts)
+    n = stop - start + 1
+    bounds = [start]
+    for i in range(1, parts):
+        b = start + n * i // parts
+        b += (2 - b) % 30          # next value == 2 (mod 30)
+        b = min(b, stop + 1)
+        bounds.append(max(b, bounds[-1]))
+    bounds.append(stop + 1)
+    return [(a, b - 1) for a, b in zip(bounds, bounds[1:]) if a <= b - 1]

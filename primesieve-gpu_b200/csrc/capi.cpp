@@ -1,0 +1,202 @@
+// capi.cpp -- the extern "C" psg_* boundary over psg::Engine.
+//
+// Status codes in, no exceptions out; a thread-local message for the last
+// failure. Each context serialises its own calls with a mutex (the reference
+// serialises every GPU call with one global mutex, src/gpu/GpuSieve.cpp:27).
+#include "../../include/psgpu.h"
+#include "engine.hpp"
+
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+struct psg_context {
+  psg::Engine engine;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string t_last_error;
+
+int fail(int status, const std::string& msg) {
+  t_last_error = msg;
+  return status;
+}
+
+psg::EngineConfig to_engine(const psg_config* c) {
+  psg::EngineConfig e;
+  if (!c) return e;
+  e.seg_bytes = c->seg_bytes;
+  e.block = c->block;
+  e.ctas_per_sm = c->ctas_per_sm;
+  e.small_limit = c->small_limit;
+  e.big_limit = c->big_limit;
+  e.window_segments = c->window_segments;
+  e.bucket_lists = c->bucket_lists;
+  e.presieve = c->presieve;
+  e.segments_per_launch = c->segments_per_launch;
+  return e;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* psg_version(void) { return "primesieve-b200 1.0 (primesieve 12.16 count API)"; }
+
+const char* psg_last_error(void) { return t_last_error.c_str(); }
+
+const char* psg_status_string(int s) {
+  switch (s) {
+    case PSG_OK: return "ok";
+    case PSG_ERR_ARG: return "invalid argument";
+    case PSG_ERR_NO_DEVICE: return "no usable CUDA device";
+    case PSG_ERR_CUDA: return "CUDA error";
+    case PSG_ERR_NOMEM: return "out of memory";
+    case PSG_ERR_LIMIT: return "request beyond a supported limit";
+    case PSG_ERR_INTERNAL: return "internal error";
+    case PSG_ERR_TIMEOUT: return "timed out";
+    case PSG_ERR_CLOSED: return "closed";
+    default: return "unknown status";
+  }
+}
+
+int psg_device_count(int* count) {
+  if (!count) return fail(PSG_ERR_ARG, "count is NULL");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    return PSG_OK;      // no driver / no device: zero devices
+  }
+  *count = n;
+  return PSG_OK;
+}
+
+int psg_device_describe(int index, char* buf, size_t len) {
+  if (!buf || len == 0) return fail(PSG_ERR_ARG, "buffer is NULL");
+  int n = 0;
+  psg_device_count(&n);
+  if (index < 0 || index >= n) return fail(PSG_ERR_NO_DEVICE, "GPU device index out of range");
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, index) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PSG_ERR_CUDA, "cudaGetDeviceProperties failed");
+  }
+  std::snprintf(buf, len,
+                "[%d] CUDA: %s (CUDA compute %d.%d)\n"
+                "      %d compute units, %d MHz, %llu MiB global, %llu KiB local, max work-group %d",
+                index, p.name, p.major, p.minor, p.multiProcessorCount, p.clockRate / 1000,
+                (unsigned long long) (p.totalGlobalMem >> 20),
+                (unsigned long long) (p.sharedMemPerBlockOptin >> 10), p.maxThreadsPerBlock);
+  return PSG_OK;
+}
+
+int psg_init(int device, const psg_config* cfg, psg_context** out) {
+  if (!out) return fail(PSG_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  std::unique_ptr<psg_context> ctx(new (std::nothrow) psg_context());
+  if (!ctx) return fail(PSG_ERR_NOMEM, "cannot allocate context");
+  std::string err;
+  int rc = ctx->engine.init(device, to_engine(cfg), err);
+  if (rc) return fail(rc, err);
+  *out = ctx.release();
+  return PSG_OK;
+}
+
+void psg_destroy(psg_context* ctx) { delete ctx; }
+
+int psg_get_config(const psg_context* ctx, psg_config* out) {
+  if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
+  const psg::EngineConfig& c = ctx->engine.config();
+  std::memset(out, 0, sizeof *out);
+  out->seg_bytes = ctx->engine.seg_bytes();
+  out->block = ctx->engine.block();
+  out->ctas_per_sm = ctx->engine.grid() / (uint32_t) ctx->engine.props().multiProcessorCount;
+  out->small_limit = c.small_limit;
+  out->big_limit = c.big_limit;
+  out->window_segments = c.window_segments;
+  out->bucket_lists = c.bucket_lists;
+  out->presieve = c.presieve;
+  out->segments_per_launch = c.segments_per_launch;
+  return PSG_OK;
+}
+
+int psg_describe(const psg_context* ctx, char* buf, size_t len) {
+  if (!ctx || !buf || !len) return fail(PSG_ERR_ARG, "NULL argument");
+  std::snprintf(buf, len, "%s", ctx->engine.describe().c_str());
+  return PSG_OK;
+}
+
+int psg_count(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6]) {
+  if (!ctx || !counts) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  int rc = ctx->engine.count(start, stop, kinds, counts, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
+                    uint64_t* dev_counts, void* stream) {
+  if (!ctx || !dev_counts) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  int rc = ctx->engine.count_async(start, stop, kinds, reinterpret_cast<unsigned long long*>(dev_counts),
+                                   static_cast<cudaStream_t>(stream), err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n, uint64_t* counts) {
+  if (!ctx || (n && (!ranges || !counts))) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  for (size_t i = 0; i < n; i++) {
+    int rc = ctx->engine.count(ranges[i].start, ranges[i].stop, ranges[i].kinds, counts + 6 * i, err);
+    if (rc) return fail(rc, err);
+  }
+  return PSG_OK;
+}
+
+int psg_prepare(psg_context* ctx, uint64_t stop) {
+  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  int rc = ctx->engine.prepare(stop, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_set_profiling(psg_context* ctx, int on) {
+  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->engine.set_profiling(on != 0);
+  return PSG_OK;
+}
+
+int psg_kernel_stats(psg_context* ctx, const char** names, uint64_t* launches, double* ms,
+                     size_t cap, size_t* n) {
+  if (!ctx || !n) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::vector<psg::KernelStat> st = ctx->engine.kernel_stats();
+  *n = st.size();
+  for (size_t i = 0; i < st.size() && i < cap; i++) {
+    if (names) names[i] = st[i].name;
+    if (launches) launches[i] = st[i].launches;
+    if (ms) ms[i] = st[i].ms;
+  }
+  return PSG_OK;
+}
+
+int psg_reset_kernel_stats(psg_context* ctx) {
+  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->engine.reset_kernel_stats();
+  return PSG_OK;
+}
+
+} // extern "C"

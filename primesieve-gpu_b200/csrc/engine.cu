@@ -1,0 +1,561 @@
+// engine.cu -- host engine: tables, sieving primes, windows and launches.
+#include "engine.hpp"
+#include "sieve_kernel.cuh"
+#include "bucket_kernel.cuh"
+#include "../../include/psgpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace psg {
+
+namespace {
+
+#define PSG_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return PSG_ERR_CUDA;                                                      \
+    }                                                                           \
+  } while (0)
+
+uint32_t isqrt64(uint64_t x) {
+  uint64_t r = (uint64_t) std::sqrt((double) x);
+  while (r > 0 && (r > 0xffffffffull || r * r > x)) r--;
+  while (r + 1 <= 0xffffffffull && (r + 1) * (r + 1) <= x) r++;
+  return (uint32_t) r;
+}
+
+// Primes in (after, limit], limit < 2^32, by an odd-only segmented sieve.
+void host_primes(uint32_t after, uint32_t limit, std::vector<uint32_t>& out) {
+  if (limit <= after) return;
+  const uint32_t r = isqrt64(limit);
+  std::vector<uint8_t> small(r + 1, 0);
+  std::vector<uint32_t> base;
+  for (uint32_t i = 3; i <= r; i += 2) {
+    if (small[i]) continue;
+    base.push_back(i);
+    for (uint64_t j = (uint64_t) i * i; j <= r; j += 2ull * i) small[j] = 1;
+  }
+  if (after < 2 && limit >= 2) out.push_back(2);
+  const uint64_t SEG = 1u << 18;               // odd numbers per segment
+  std::vector<uint8_t> seg(SEG);
+  std::vector<uint64_t> next(base.size(), 0);
+  uint64_t lo0 = std::max<uint64_t>(3, (uint64_t) after + 1) | 1ull;
+  for (size_t k = 0; k < base.size(); k++) {
+    const uint64_t p = base[k];
+    uint64_t m = std::max<uint64_t>(p * p, (lo0 + p - 1) / p * p);
+    if ((m & 1) == 0) m += p;
+    next[k] = m;
+  }
+  for (uint64_t lo = lo0; lo <= limit; lo += 2 * SEG) {
+    const uint64_t hi = std::min<uint64_t>(lo + 2 * SEG - 2, limit);
+    const uint64_t cnt = (hi - lo) / 2 + 1;
+    std::memset(seg.data(), 0, cnt);
+    for (size_t k = 0; k < base.size(); k++) {
+      const uint64_t p = base[k];
+      if (p * p > hi) break;
+      uint64_t m = next[k];
+      for (; m <= hi; m += 2 * p) seg[(m - lo) >> 1] = 1;
+      next[k] = m;
+    }
+    for (uint64_t i = 0; i < cnt; i++)
+      if (!seg[i]) out.push_back((uint32_t) (lo + 2 * i));
+  }
+}
+
+__global__ void recip_kernel(const uint32_t* __restrict__ p, uint64_t* __restrict__ r, size_t n) {
+  for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n;
+       i += (size_t) gridDim.x * blockDim.x)
+    r[i] = 0xffffffffffffffffull / p[i];
+}
+
+__global__ void add_counts_kernel(unsigned long long* c, unsigned long long a0, unsigned long long a1,
+                                  unsigned long long a2, unsigned long long a3,
+                                  unsigned long long a4, unsigned long long a5) {
+  if (threadIdx.x == 0) {
+    c[0] += a0; c[1] += a1; c[2] += a2; c[3] += a3; c[4] += a4; c[5] += a5;
+  }
+}
+
+// The primes 2, 3, 5 and the k-tuplets containing them cannot be stored in
+// the wheel-30 bit array; they are counted from this table when
+// start <= 5 (reference src/gpu/GpuSieve.cpp:149-169,
+// src/PrimeSieveClass.cpp:38-48).
+void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]) {
+  struct T { uint64_t first, last; int kind; };
+  static const T tab[8] = { { 2, 2, 0 }, { 3, 3, 0 }, { 5, 5, 0 }, { 3, 5, 1 },
+                            { 5, 7, 1 }, { 5, 11, 2 }, { 5, 13, 3 }, { 5, 17, 4 } };
+  if (start > 5) return;
+  for (const T& t : tab)
+    if (((kinds >> t.kind) & 1u) && t.first >= start && t.last <= stop) out[t.kind]++;
+}
+
+template <int BLOCK>
+void set_smem_attrs(uint32_t bytes) {
+  cudaFuncSetAttribute(sieve_count_kernel<BLOCK, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
+  cudaFuncSetAttribute(sieve_count_kernel<BLOCK, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
+}
+
+template <int BLOCK>
+int occupancy(uint32_t bytes) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sieve_count_kernel<BLOCK, true>, BLOCK, bytes);
+  return n;
+}
+
+cudaError_t launch_sieve(uint32_t block, bool all, uint32_t grid, uint32_t smem,
+                         cudaStream_t st, const SieveArgs& a) {
+  switch (block) {
+    case 256:
+      if (all) sieve_count_kernel<256, true><<<grid, 256, smem, st>>>(a);
+      else     sieve_count_kernel<256, false><<<grid, 256, smem, st>>>(a);
+      break;
+    case 1024:
+      if (all) sieve_count_kernel<1024, true><<<grid, 1024, smem, st>>>(a);
+      else     sieve_count_kernel<1024, false><<<grid, 1024, smem, st>>>(a);
+      break;
+    default:
+      if (all) sieve_count_kernel<512, true><<<grid, 512, smem, st>>>(a);
+      else     sieve_count_kernel<512, false><<<grid, 512, smem, st>>>(a);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+} // namespace
+
+Engine::~Engine() {
+  if (device_ < 0) return;
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (auto& t : timed_)
+    for (auto& e : t.ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  cudaFree(d_pat_);
+  cudaFree(d_primes_);
+  cudaFree(d_recip_);
+  cudaFree(d_entries_);
+  cudaFree(d_bcounts_);
+  cudaFree(d_list_off_);
+  cudaFree(d_list_cap_);
+  cudaFree(d_overflow_);
+  cudaFree(d_counts_);
+  if (h_counts_) cudaFreeHost(h_counts_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    err = "no CUDA device found";
+    return PSG_ERR_NO_DEVICE;
+  }
+  if (device < 0) {
+    int best = 0, best_sm = -1;
+    for (int i = 0; i < n; i++) {
+      int sm = 0;
+      cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, i);
+      if (sm > best_sm) { best_sm = sm; best = i; }
+    }
+    device = best;
+  }
+  if (device >= n) {
+    err = "GPU device index out of range";
+    return PSG_ERR_NO_DEVICE;
+  }
+  device_ = device;
+  cfg_ = cfg;
+  PSG_CUDA(cudaSetDevice(device_));
+  PSG_CUDA(cudaGetDeviceProperties(&prop_, device_));
+  if (prop_.major < 10) {
+    err = "this build contains sm_100a code only; device " + std::string(prop_.name) +
+          " has compute capability " + std::to_string(prop_.major) + "." + std::to_string(prop_.minor);
+    return PSG_ERR_NO_DEVICE;
+  }
+  PSG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+  // ---- geometry ------------------------------------------------------------
+  block_ = cfg.block ? cfg.block : 512;
+  if (block_ != 256 && block_ != 512 && block_ != 1024) {
+    err = "block must be 256, 512 or 1024";
+    return PSG_ERR_ARG;
+  }
+  const uint32_t smem_optin = (uint32_t) prop_.sharedMemPerBlockOptin;
+  seg_bytes_ = cfg.seg_bytes ? cfg.seg_bytes : 65536u;
+  seg_bytes_ = std::min(seg_bytes_, smem_optin);
+  seg_bytes_ &= ~(16u * block_ - 1u);          // whole 16-byte chunks per thread
+  if (seg_bytes_ < 16u * block_) {
+    err = "segment too small for the block size";
+    return PSG_ERR_ARG;
+  }
+  switch (block_) {
+    case 256: set_smem_attrs<256>(seg_bytes_); break;
+    case 1024: set_smem_attrs<1024>(seg_bytes_); break;
+    default: set_smem_attrs<512>(seg_bytes_); break;
+  }
+  int occ = block_ == 256 ? occupancy<256>(seg_bytes_)
+          : block_ == 1024 ? occupancy<1024>(seg_bytes_) : occupancy<512>(seg_bytes_);
+  if (occ < 1) {
+    err = "sieve kernel cannot be resident with this segment/block size";
+    return PSG_ERR_ARG;
+  }
+  if (cfg.ctas_per_sm) occ = std::min<int>(occ, (int) cfg.ctas_per_sm);
+  grid_ = (uint32_t) (prop_.multiProcessorCount * occ);
+
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  small_limit_ = cfg.small_limit ? cfg.small_limit : seg_bytes_ / 8u;
+  big_limit_ = cfg.big_limit ? cfg.big_limit : (uint32_t) std::min<uint64_t>(span / 10u, 0xffffffffull);
+  if (big_limit_ < small_limit_) big_limit_ = small_limit_;
+  window_ = cfg.window_segments ? cfg.window_segments : grid_ * 4u;
+  window_ = std::min<uint32_t>(window_, 12000u);     // counters must fit in smem
+  lists_ = cfg.bucket_lists ? cfg.bucket_lists : (uint32_t) prop_.multiProcessorCount * 2u;
+  cudaFuncSetAttribute(bucket_fill_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) (window_ * sizeof(uint32_t)));
+
+  PSG_CUDA(cudaMalloc(&d_counts_, 6 * sizeof(unsigned long long)));
+  PSG_CUDA(cudaMalloc(&d_overflow_, sizeof(uint32_t)));
+  PSG_CUDA(cudaMemset(d_overflow_, 0, sizeof(uint32_t)));
+  PSG_CUDA(cudaMallocHost(&h_counts_, 8 * sizeof(unsigned long long)));
+
+  if (cfg.presieve == 0) {
+    presieve_max_ = 5;
+  } else {
+    int rc = build_presieve(err);
+    if (rc) return rc;
+  }
+  return PSG_OK;
+}
+
+// Pre-sieve pattern tables. A group's pattern has one byte per wheel-30 byte
+// over one period (the product of the group's primes); a bit is cleared iff
+// its value is a multiple of a group prime. Stored as 16 copies shifted by
+// 0..15 bytes so that any 16 consecutive pattern bytes are one aligned
+// 128-bit load. (Reference: 4-byte sliding windows,
+// src/gpu/GpuTables.cpp:31-130; the groups here reach 59.)
+int Engine::build_presieve(std::string& err) {
+  groups_ = { { 7, 11, 13, 17 }, { 19, 23, 29, 31 }, { 37, 41, 43 }, { 47, 53, 59 } };
+  size_t total = 0;
+  pat_off_.clear(); pat_period_.clear(); pat_stride_.clear(); presieve_primes_.clear();
+  for (auto& g : groups_) {
+    uint64_t P = 1;
+    for (uint32_t p : g) { P *= p; presieve_primes_.push_back(p); presieve_max_ = std::max(presieve_max_, p); }
+    const uint32_t stride = (uint32_t) ((P + 15 + 15) & ~15ull);
+    pat_off_.push_back(total);
+    pat_period_.push_back((uint32_t) P);
+    pat_stride_.push_back(stride);
+    total += 16ull * stride;
+  }
+  std::vector<uint8_t> host(total, 0);
+  for (size_t t = 0; t < groups_.size(); t++) {
+    const uint32_t P = pat_period_[t];
+    std::vector<uint8_t> pat(P, 0xff);
+    for (uint32_t p : groups_[t]) {
+      // multiples of p coprime to 30 inside [0, 30 P)
+      for (uint64_t m = p; m < 30ull * P; m += 2ull * p) {
+        if (m % 3 == 0 || m % 5 == 0) continue;
+        const uint64_t byte = (m - 7) / 30;               // value 30*byte + off
+        const uint32_t bit = residue_to_bit((uint32_t) (m % 30));
+        pat[byte] &= (uint8_t) ~(1u << bit);
+      }
+    }
+    for (uint32_t k = 0; k < 16; k++) {
+      uint8_t* copy = host.data() + pat_off_[t] + (size_t) k * pat_stride_[t];
+      for (uint32_t i = 0; i < pat_stride_[t]; i++) copy[i] = pat[(i + k) % P];
+    }
+  }
+  PSG_CUDA(cudaMalloc(&d_pat_, total));
+  PSG_CUDA(cudaMemcpy(d_pat_, host.data(), total, cudaMemcpyHostToDevice));
+  return PSG_OK;
+}
+
+int Engine::ensure_primes(uint64_t limit, std::string& err) {
+  if (limit <= primes_upto_ && d_primes_) return PSG_OK;
+  // grow geometrically so repeated calls with rising stops stay cheap
+  uint64_t target = std::max<uint64_t>(limit, std::min<uint64_t>(primes_upto_ * 2, 0xffffffffull));
+  target = std::max<uint64_t>(target, 1u << 16);
+  target = std::min<uint64_t>(target, 0xffffffffull);
+  const uint32_t after = std::max<uint32_t>(presieve_max_, (uint32_t) std::min<uint64_t>(primes_upto_, 0xffffffffull));
+  std::vector<uint32_t> more;
+  host_primes(after, (uint32_t) target, more);
+  const size_t old_n = h_primes_.size();
+  h_primes_.insert(h_primes_.end(), more.begin(), more.end());
+  primes_upto_ = target;
+  const size_t n = h_primes_.size();
+  if (n > d_primes_cap_) {
+    uint32_t* np = nullptr; uint64_t* nr = nullptr;
+    size_t cap = std::max<size_t>(n, 1024);
+    PSG_CUDA(cudaMalloc(&np, cap * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&nr, cap * sizeof(uint64_t)));
+    if (old_n) {
+      PSG_CUDA(cudaMemcpyAsync(np, d_primes_, old_n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+      PSG_CUDA(cudaMemcpyAsync(nr, d_recip_, old_n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream_));
+    }
+    PSG_CUDA(cudaStreamSynchronize(stream_));
+    cudaFree(d_primes_); cudaFree(d_recip_);
+    d_primes_ = np; d_recip_ = nr; d_primes_cap_ = cap;
+  }
+  if (n > old_n) {
+    PSG_CUDA(cudaMemcpyAsync(d_primes_ + old_n, h_primes_.data() + old_n, (n - old_n) * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, stream_));
+    const size_t m = n - old_n;
+    const uint32_t g = (uint32_t) std::min<size_t>((m + 255) / 256, 4096);
+    recip_kernel<<<g, 256, 0, stream_>>>(d_primes_ + old_n, d_recip_ + old_n, m);
+    PSG_CUDA(cudaGetLastError());
+    PSG_CUDA(cudaStreamSynchronize(stream_));
+  }
+  return PSG_OK;
+}
+
+int Engine::prepare(uint64_t stop, std::string& err) {
+  PSG_CUDA(cudaSetDevice(device_));
+  return ensure_primes(std::max<uint32_t>(isqrt64(stop), 7u), err);
+}
+
+// Bucket lists for big primes primes[first, last): one list per bucket CTA
+// (a contiguous chunk of primes), capacity = expected entries per segment
+// + 6 sigma + 32, all lists of one segment packed in one region.
+int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
+  if (first == bucket_first_ && last == bucket_last_ && d_entries_) return PSG_OK;
+  const uint32_t nbig = last - first;
+  const uint32_t lists = std::min<uint32_t>(lists_, nbig);
+  const uint32_t ppl = (nbig + lists - 1) / lists;
+  const double span = (double) seg_bytes_ * 30.0;
+  std::vector<uint32_t> off(lists), cap(lists);
+  uint64_t stride = 0;
+  for (uint32_t l = 0; l < lists; l++) {
+    double mu = 0;
+    const uint32_t a = first + l * ppl, b = std::min<uint32_t>(last, a + ppl);
+    for (uint32_t i = a; i < b; i++) mu += span * (8.0 / 30.0) / (double) h_primes_[i];
+    double c = (mu + 6.0 * std::sqrt(mu) + 32.0) * cap_scale_;
+    uint32_t ci = (uint32_t) std::ceil(c);
+    ci = (ci + 3u) & ~3u;
+    off[l] = (uint32_t) stride;
+    cap[l] = ci;
+    stride += ci;
+  }
+  if (stride > 0xffffffffull) { err = "bucket region too large"; return PSG_ERR_LIMIT; }
+  const size_t need_entries = (size_t) stride * window_;
+  if (need_entries > entries_cap_) {
+    cudaFree(d_entries_); d_entries_ = nullptr; entries_cap_ = 0;
+    if (cudaMalloc(&d_entries_, need_entries * sizeof(uint32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      err = "cannot allocate " + std::to_string(need_entries * 4 >> 20) + " MiB of bucket storage";
+      return PSG_ERR_NOMEM;
+    }
+    entries_cap_ = need_entries;
+  }
+  const size_t need_counts = (size_t) lists * window_;
+  if (need_counts > bcounts_cap_) {
+    cudaFree(d_bcounts_); d_bcounts_ = nullptr;
+    PSG_CUDA(cudaMalloc(&d_bcounts_, need_counts * sizeof(uint32_t)));
+    bcounts_cap_ = need_counts;
+  }
+  if (lists > lists_cap_) {
+    cudaFree(d_list_off_); cudaFree(d_list_cap_);
+    PSG_CUDA(cudaMalloc(&d_list_off_, lists * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&d_list_cap_, lists * sizeof(uint32_t)));
+    lists_cap_ = lists;
+  }
+  PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+  PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+  PSG_CUDA(cudaStreamSynchronize(stream_));
+  seg_stride_ = stride;
+  bucket_first_ = first;
+  bucket_last_ = last;
+  primes_per_list_ = ppl;
+  active_lists_ = lists;
+  return PSG_OK;
+}
+
+void Engine::timed_begin(int which, cudaStream_t st) {
+  if (!profiling_) return;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a); cudaEventCreate(&b);
+  cudaEventRecord(a, st);
+  timed_[which].ev.emplace_back(a, b);
+}
+
+void Engine::timed_end(int which, cudaStream_t st) {
+  if (!profiling_) return;
+  cudaEventRecord(timed_[which].ev.back().second, st);
+}
+
+std::vector<KernelStat> Engine::kernel_stats() {
+  std::vector<KernelStat> out;
+  cudaSetDevice(device_);
+  for (auto& t : timed_) {
+    for (auto& e : t.ev) {
+      cudaEventSynchronize(e.second);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e.first, e.second);
+      t.ms += ms;
+      t.launches++;
+      cudaEventDestroy(e.first); cudaEventDestroy(e.second);
+    }
+    t.ev.clear();
+    KernelStat k; k.name = t.name; k.launches = t.launches; k.ms = t.ms;
+    out.push_back(k);
+  }
+  return out;
+}
+
+void Engine::reset_kernel_stats() {
+  kernel_stats();
+  for (auto& t : timed_) { t.launches = 0; t.ms = 0; }
+}
+
+int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
+                cudaStream_t st, std::string& err) {
+  // lo >= 7, lo <= hi
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  // byteRemainder (reference src/Erat.cpp:231-237, CudaBackend.cpp:457)
+  const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
+  const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
+  const uint32_t sq = isqrt64(hi);
+  int rc = ensure_primes(std::max<uint32_t>(sq, 7u), err);
+  if (rc) return rc;
+
+  const auto upto = [&](uint64_t v) {
+    return (uint32_t) (std::upper_bound(h_primes_.begin(), h_primes_.end(), (uint32_t) std::min<uint64_t>(v, 0xffffffffull)) - h_primes_.begin());
+  };
+  const auto below = [&](uint64_t v) {
+    return (uint32_t) (std::lower_bound(h_primes_.begin(), h_primes_.end(), (uint32_t) std::min<uint64_t>(v, 0xffffffffull)) - h_primes_.begin());
+  };
+  const uint32_t n_total = upto(sq);
+  const uint32_t n_small = std::min(below(small_limit_), n_total);
+  const uint32_t n_med = std::min(below(big_limit_), n_total);
+  const bool use_buckets = n_med < n_total;
+  if (use_buckets) {
+    rc = ensure_buckets(n_med, n_total, err);
+    if (rc) return rc;
+  }
+
+  SieveArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.lo = lo; a.hi = hi;
+  a.seg_bytes = seg_bytes_;
+  a.num_tables = (uint32_t) pat_period_.size();
+  for (size_t t = 0; t < pat_period_.size(); t++) {
+    a.pat_base[t] = d_pat_ + pat_off_[t];
+    a.pat_period[t] = pat_period_[t];
+    a.pat_stride[t] = pat_stride_[t];
+    a.pat_rcp[t] = 0xffffffffffffffffull / pat_period_[t];
+  }
+  a.num_presieve_primes = (uint32_t) presieve_primes_.size();
+  for (size_t i = 0; i < presieve_primes_.size() && i < (size_t) kMaxPresievePrimes; i++)
+    a.presieve_primes[i] = presieve_primes_[i];
+  a.presieve_max = presieve_max_;
+  a.primes = d_primes_;
+  a.recip = d_recip_;
+  a.n_small = n_small;
+  a.n_primes = n_med;
+  a.kinds = kinds;
+  a.counts = dev_counts;
+  const bool all = (kinds & ~1u) != 0;
+
+  const uint64_t step = use_buckets ? window_
+                      : (cfg_.segments_per_launch ? cfg_.segments_per_launch : nseg);
+  for (uint64_t s0 = 0; s0 < nseg; s0 += step) {
+    const uint64_t ns = std::min<uint64_t>(step, nseg - s0);
+    const uint64_t win_low = seg_low0 + s0 * span;
+    a.seg_low0 = win_low;
+    a.num_segments = ns;
+    if (use_buckets) {
+      BucketArgs b;
+      std::memset(&b, 0, sizeof b);
+      b.win_low = win_low;
+      b.win_segments = (uint32_t) ns;
+      b.seg_bytes = seg_bytes_;
+      b.seg_rcp = 0xffffffffffffffffull / seg_bytes_;
+      b.primes = d_primes_;
+      b.recip = d_recip_;
+      b.first = bucket_first_;
+      b.last = bucket_last_;
+      b.primes_per_list = primes_per_list_;
+      b.num_lists = active_lists_;
+      b.list_off = d_list_off_;
+      b.list_cap = d_list_cap_;
+      b.seg_stride = seg_stride_;
+      b.entries = d_entries_;
+      b.counts = d_bcounts_;
+      b.overflow = d_overflow_;
+      timed_begin(1, st);
+      bucket_fill_kernel<256><<<active_lists_, 256, (size_t) ns * sizeof(uint32_t), st>>>(b);
+      timed_end(1, st);
+      PSG_CUDA(cudaGetLastError());
+      a.bucket_entries = d_entries_;
+      a.bucket_counts = d_bcounts_;
+      a.bucket_list_off = d_list_off_;
+      a.bucket_seg_stride = seg_stride_;
+      a.num_bucket_lists = active_lists_;
+    }
+    const uint32_t g = (uint32_t) std::min<uint64_t>(grid_, ns);
+    timed_begin(0, st);
+    cudaError_t e = launch_sieve(block_, all, g, seg_bytes_, st, a);
+    timed_end(0, st);
+    if (e != cudaSuccess) {
+      err = std::string("sieve kernel launch: ") + cudaGetErrorString(e);
+      return PSG_ERR_CUDA;
+    }
+  }
+  return PSG_OK;
+}
+
+int Engine::count_async(uint64_t start, uint64_t stop, uint32_t kinds,
+                        unsigned long long* dev_counts, cudaStream_t stream, std::string& err) {
+  PSG_CUDA(cudaSetDevice(device_));
+  cudaStream_t st = stream ? stream : stream_;
+  kinds &= 0x3fu;
+  if (start > stop || kinds == 0) return PSG_OK;
+  uint64_t tab[6] = { 0, 0, 0, 0, 0, 0 };
+  small_table(start, stop, kinds, tab);
+  if (tab[0] | tab[1] | tab[2] | tab[3] | tab[4]) {
+    add_counts_kernel<<<1, 32, 0, st>>>(dev_counts, tab[0], tab[1], tab[2], tab[3], tab[4], tab[5]);
+    PSG_CUDA(cudaGetLastError());
+  }
+  if (stop < 7) return PSG_OK;
+  const uint64_t lo = std::max<uint64_t>(start, 7);
+  return run(lo, stop, kinds, dev_counts, st, err);
+}
+
+int Engine::count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6], std::string& err) {
+  for (int i = 0; i < 6; i++) counts[i] = 0;
+  PSG_CUDA(cudaSetDevice(device_));
+  kinds &= 0x3fu;
+  if (start > stop || kinds == 0) return PSG_OK;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    PSG_CUDA(cudaMemsetAsync(d_counts_, 0, 6 * sizeof(unsigned long long), stream_));
+    PSG_CUDA(cudaMemsetAsync(d_overflow_, 0, sizeof(uint32_t), stream_));
+    int rc = count_async(start, stop, kinds, d_counts_, stream_, err);
+    if (rc) return rc;
+    PSG_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+    PSG_CUDA(cudaMemcpyAsync(h_counts_ + 6, d_overflow_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    PSG_CUDA(cudaStreamSynchronize(stream_));
+    const uint32_t overflow = (uint32_t) (h_counts_[6] & 0xffffffffu);
+    if (!overflow) {
+      for (int i = 0; i < 6; i++) counts[i] = ((kinds >> i) & 1u) ? h_counts_[i] : 0;
+      return PSG_OK;
+    }
+    // a bucket list overflowed: recount with larger lists
+    overflow_retries_++;
+    cap_scale_ *= 2.0;
+    bucket_first_ = bucket_last_ = 0;
+  }
+  err = "bucket lists kept overflowing";
+  return PSG_ERR_INTERNAL;
+}
+
+std::string Engine::describe() const {
+  char buf[512];
+  std::snprintf(buf, sizeof buf,
+                "[%d] CUDA: %s (compute %d.%d), %d SMs, %llu MiB, segment %u B x %u threads, grid %u",
+                device_, prop_.name, prop_.major, prop_.minor, prop_.multiProcessorCount,
+                (unsigned long long) (prop_.totalGlobalMem >> 20), seg_bytes_, block_, grid_);
+  return buf;
+}
+
+} // namespace psg

@@ -1,0 +1,127 @@
+// engine.hpp -- host side of the B200 counting engine.
+//
+// An Engine owns one CUDA device context's worth of state: a stream, the
+// pre-sieve pattern tables, the sieving-prime table (+ reciprocals), the
+// bucket storage of the big-prime sieve and the count accumulators. It is
+// the replacement of the reference's CudaBackend (src/gpu/cuda/CudaBackend.cpp)
+// behind the GpuBackend::count(lo, hi, countType) contract
+// (src/gpu/GpuBackend.hpp:66-69), extended to all six counts in one pass.
+#pragma once
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include <mutex>
+#include <cuda_runtime.h>
+
+namespace psg {
+
+struct EngineConfig {
+  uint32_t seg_bytes = 0;        // shared-memory segment per CTA; 0 = auto
+  uint32_t block = 0;            // threads per CTA (256/512/1024); 0 = auto
+  uint32_t ctas_per_sm = 0;      // resident sieve CTAs per SM; 0 = max
+  uint32_t small_limit = 0;      // primes below: warp-cooperative; 0 = auto
+  uint32_t big_limit = 0;        // primes from: bucket sieve; 0 = auto
+  uint32_t window_segments = 0;  // segments per bucket window; 0 = auto
+  uint32_t bucket_lists = 0;     // lists (bucket CTAs) per segment; 0 = auto
+  uint32_t presieve = 1;         // pre-sieve with pattern tables
+  uint32_t segments_per_launch = 0; // cap on segments per sieve launch; 0 = auto
+};
+
+struct KernelStat {
+  const char* name;
+  uint64_t launches = 0;
+  double ms = 0.0;
+};
+
+class Engine {
+public:
+  Engine() = default;
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Returns 0 or a psg status code; err gets a message.
+  int init(int device, const EngineConfig& cfg, std::string& err);
+
+  // Count the requested kinds (bit i of kinds = counts[i]) in [start, stop].
+  // Results are added to dev_counts (device, 6 x u64) on `stream`
+  // (nullptr: the engine's stream). No host synchronisation.
+  int count_async(uint64_t start, uint64_t stop, uint32_t kinds,
+                  unsigned long long* dev_counts, cudaStream_t stream, std::string& err);
+
+  // Synchronous host-result version (counts[6] overwritten).
+  int count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6], std::string& err);
+
+  // Make sure the sieving-prime table covers sqrt(stop) (host work + upload).
+  int prepare(uint64_t stop, std::string& err);
+
+  int device() const { return device_; }
+  const cudaDeviceProp& props() const { return prop_; }
+  cudaStream_t stream() const { return stream_; }
+  const EngineConfig& config() const { return cfg_; }
+  uint32_t seg_bytes() const { return seg_bytes_; }
+  uint32_t block() const { return block_; }
+  uint32_t grid() const { return grid_; }
+  std::string describe() const;
+
+  // Per-kernel CUDA-event timing (off by default).
+  void set_profiling(bool on) { profiling_ = on; }
+  std::vector<KernelStat> kernel_stats();
+  void reset_kernel_stats();
+  uint64_t overflow_retries() const { return overflow_retries_; }
+
+private:
+  int build_presieve(std::string& err);
+  int ensure_primes(uint64_t limit, std::string& err);
+  int ensure_buckets(uint32_t first_big, uint32_t last_big, std::string& err);
+  int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
+          cudaStream_t st, std::string& err);
+  void timed_begin(int which, cudaStream_t st);
+  void timed_end(int which, cudaStream_t st);
+
+  int device_ = -1;
+  cudaDeviceProp prop_{};
+  cudaStream_t stream_ = nullptr;
+  EngineConfig cfg_;
+  uint32_t seg_bytes_ = 0, block_ = 0, grid_ = 0, bucket_block_ = 256;
+  uint32_t small_limit_ = 0, big_limit_ = 0, window_ = 0, lists_ = 0;
+
+  // pre-sieve tables
+  std::vector<std::vector<uint32_t>> groups_;
+  uint8_t* d_pat_ = nullptr;
+  std::vector<size_t> pat_off_;
+  std::vector<uint32_t> pat_period_, pat_stride_;
+  std::vector<uint32_t> presieve_primes_;
+  uint32_t presieve_max_ = 0;
+
+  // sieving primes > presieve_max_, ascending
+  std::vector<uint32_t> h_primes_;
+  uint64_t primes_upto_ = 0;
+  uint32_t* d_primes_ = nullptr;
+  uint64_t* d_recip_ = nullptr;
+  size_t d_primes_cap_ = 0;
+
+  // bucket storage
+  uint32_t* d_entries_ = nullptr;
+  size_t entries_cap_ = 0;
+  uint32_t* d_bcounts_ = nullptr;
+  size_t bcounts_cap_ = 0;
+  uint32_t* d_list_off_ = nullptr;
+  uint32_t* d_list_cap_ = nullptr;
+  size_t lists_cap_ = 0;
+  uint64_t seg_stride_ = 0;
+  uint32_t bucket_first_ = 0, bucket_last_ = 0, primes_per_list_ = 0, active_lists_ = 0;
+  double cap_scale_ = 1.0;
+  uint32_t* d_overflow_ = nullptr;
+  uint64_t overflow_retries_ = 0;
+
+  unsigned long long* d_counts_ = nullptr;
+  unsigned long long* h_counts_ = nullptr;   // pinned
+
+  // profiling
+  bool profiling_ = false;
+  struct Timed { const char* name; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev; uint64_t launches = 0; double ms = 0; };
+  Timed timed_[2] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 } };
+};
+
+} // namespace psg

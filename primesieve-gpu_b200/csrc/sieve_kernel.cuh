@@ -1,0 +1,311 @@
+// sieve_kernel.cuh -- the segment sieve kernel (sm_100a).
+//
+// One CTA sieves one wheel-30 segment at a time in shared memory and loops
+// over segments (persistent grid). Per segment:
+//   1. pre-sieve : AND of the pre-sieve patterns, 16 bytes per thread per
+//                  step, read as aligned 128-bit loads from 16 pre-shifted
+//                  copies of each pattern (L2-resident), stored with
+//                  conflict-free 128-bit shared stores.
+//   2. small     : warp-cooperative cross-off. One warp per prime; lane
+//                  (j = lane&7, r = lane>>3) walks the multiples whose
+//                  cofactor is in class kCofactor[j] (mod 30), every 4th
+//                  one starting at phase r. Those multiples are p bytes
+//                  apart, so the lane strides 4p bytes = p words and its
+//                  bit (and byte-in-word) never changes: the inner loop is
+//                  one shared atomicAnd per crossing.
+//   3. medium    : one thread per prime, the same 8 progressions walked
+//                  one after the other (stride p bytes).
+//   4. big       : crossings streamed from the per-segment bucket lists
+//                  that the bucket kernel wrote to HBM (4-byte entries).
+//   5. count     : edge masking, __popc over the word and over shifted ANDs
+//                  for the k-tuplet start masks, warp-shuffle reduction,
+//                  one 64-bit atomicAdd per warp and kind at kernel end.
+//
+// Reference counterpart: ps_count, src/gpu/cuda/sieve.cu:157-320 (one
+// block per segment, shared-memory sieve, smem atomicAnd cross-off, byte
+// LUT count and a tree reduction into one u64 per segment).
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+#include "wheel.hpp"
+
+namespace psg {
+
+constexpr int kMaxPresieveTables = 8;
+constexpr int kMaxPresievePrimes = 24;
+
+struct SieveArgs {
+  uint64_t seg_low0;          // value base of segment 0 (multiple of 30)
+  uint64_t lo, hi;            // inclusive range, lo >= 7
+  uint64_t num_segments;
+  uint32_t seg_bytes;         // multiple of 16
+  uint32_t num_tables;
+  const uint8_t* pat_base[kMaxPresieveTables];  // 16 shifted copies each
+  uint32_t pat_period[kMaxPresieveTables];      // bytes
+  uint32_t pat_stride[kMaxPresieveTables];      // bytes per shifted copy
+  uint64_t pat_rcp[kMaxPresieveTables];         // floor((2^64-1)/period)
+  uint32_t presieve_primes[kMaxPresievePrimes]; // restored in segment 0/1
+  uint32_t num_presieve_primes;
+  uint32_t presieve_max;
+  const uint32_t* primes;     // sieving primes (> presieve_max), ascending
+  const uint64_t* recip;      // floor((2^64-1)/p) per prime
+  uint32_t n_small;           // primes[0, n_small): warp-cooperative
+  uint32_t n_primes;          // primes[n_small, n_primes): thread per prime
+  // big primes via buckets (num_bucket_lists == 0: none)
+  const uint32_t* bucket_entries;   // [segment][seg_stride] entries
+  const uint32_t* bucket_counts;    // [segment][list] number of entries
+  const uint32_t* bucket_list_off;  // [list] offset inside a segment region
+  uint64_t bucket_seg_stride;       // entries per segment region
+  uint32_t num_bucket_lists;        // lists per segment (0: no big primes)
+  uint32_t kinds;
+  unsigned long long* counts;       // [6]
+};
+
+// x mod p for p < 2^32 with a precomputed rcp = floor((2^64-1)/p).
+// q_est = mulhi(x, rcp) is at most 2 below floor(x/p) (Granlund-Montgomery
+// style reciprocal estimate), so at most two corrections are needed.
+__device__ __forceinline__ uint32_t mod_recip(uint64_t x, uint32_t p, uint64_t rcp) {
+  uint64_t q = __umul64hi(x, rcp);
+  uint64_t r = x - q * (uint64_t) p;
+  if (r >= p) r -= p;
+  if (r >= p) r -= p;
+  return (uint32_t) r;
+}
+
+// Offset d (relative to x0 = segLow + 7) of the first multiple of p that is
+// >= x0 and >= p*p, and the residue (mod 30) of its cofactor.
+// Reference: first multiple > segLow + 6 with cofactor >= p,
+// src/gpu/cuda/sieve.cu:69-99 and src/Wheel.hpp:50-89.
+__device__ __forceinline__ void first_multiple(uint64_t segLow, uint32_t p, uint64_t rcp,
+                                               uint64_t& d, uint32_t& c0) {
+  const uint64_t x0 = segLow + 7;
+  const uint64_t pp = (uint64_t) p * p;
+  const uint32_t pm = p % 30u;
+  if (x0 <= pp) {
+    d = pp - x0;
+    c0 = pm;
+  } else {
+    uint32_t r = mod_recip(x0, p, rcp);
+    uint32_t dd = r ? p - r : 0u;
+    d = dd;
+    // x0 + d = p * c  ->  c == (7 + d) * p^-1 (mod 30)
+    c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
+  }
+}
+
+__device__ __forceinline__ uint32_t cofactor_class(uint32_t j) {
+  // kCofactor[j] = {1,7,11,13,17,19,23,29}[j], 5 bits each
+  const uint64_t packed = 1ull | (7ull << 5) | (11ull << 10) | (13ull << 15) |
+                          (17ull << 20) | (19ull << 25) | (23ull << 30) | (29ull << 35);
+  return (uint32_t) ((packed >> (5 * j)) & 31u);
+}
+
+// Keep-mask of the byte whose values are base + {7..31} for the inclusive
+// window [rlo, rhi] (all relative to segLow; no wrap-around).
+__device__ __forceinline__ uint32_t byte_keep(uint64_t base, uint64_t rlo, uint64_t rhi) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const uint32_t off = (j == 0) ? 7u : (j == 1) ? 11u : (j == 2) ? 13u : (j == 3) ? 17u
+                       : (j == 4) ? 19u : (j == 5) ? 23u : (j == 6) ? 29u : 31u;
+    const uint64_t v = base + off;
+    if (v >= rlo && v <= rhi) m |= 1u << j;
+  }
+  return m;
+}
+
+template <bool ALL_KINDS>
+__device__ __forceinline__ void count_word(uint32_t w, uint32_t (&c)[6]) {
+  c[0] += __popc(w);
+  if (ALL_KINDS) {
+    const uint32_t t2 = w & (w >> 1);
+    c[1] += __popc(t2 & kTwinStart);
+    const uint32_t t3 = t2 & (w >> 2);
+    c[2] += __popc(t3 & kTripStart);
+    const uint32_t t4 = t3 & (w >> 3);
+    c[3] += __popc(t4 & kQuadStart);
+    const uint32_t t5 = t4 & (w >> 4);
+    c[4] += __popc(t5 & kQuintStart);
+    const uint32_t t6 = t5 & (w >> 5);
+    c[5] += __popc(t6 & kSextStart);
+  }
+}
+
+template <int BLOCK, bool ALL_KINDS>
+__global__ void __launch_bounds__(BLOCK)
+sieve_count_kernel(const __grid_constant__ SieveArgs a)
+{
+  extern __shared__ uint4 smem4[];
+  uint32_t* const sieve32 = reinterpret_cast<uint32_t*>(smem4);
+  constexpr int NWARPS = BLOCK / 32;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = tid & 31u;
+  const uint32_t warp = tid >> 5;
+  const uint32_t seg_bytes = a.seg_bytes;
+  const uint32_t nchunks = seg_bytes >> 4;
+  const uint32_t nwords = seg_bytes >> 2;
+  const uint64_t span = (uint64_t) seg_bytes * 30u;
+
+  uint64_t acc[6] = { 0, 0, 0, 0, 0, 0 };
+
+  for (uint64_t s = blockIdx.x; s < a.num_segments; s += gridDim.x) {
+    const uint64_t segLow = a.seg_low0 + s * span;
+
+    // ---- 1. pre-sieve --------------------------------------------------
+    {
+      const uint64_t g0 = segLow / 30u;   // global byte index of byte 0
+      uint32_t phase[kMaxPresieveTables], step[kMaxPresieveTables];
+#pragma unroll
+      for (int t = 0; t < kMaxPresieveTables; t++) {
+        if (t < (int) a.num_tables) {
+          const uint32_t P = a.pat_period[t];
+          phase[t] = mod_recip(g0 + 16ull * tid, P, a.pat_rcp[t]);
+          step[t] = (16u * BLOCK) % P;
+        }
+      }
+      for (uint32_t c = tid; c < nchunks; c += BLOCK) {
+        uint4 v = make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+        for (int t = 0; t < kMaxPresieveTables; t++) {
+          if (t < (int) a.num_tables) {
+            const uint32_t ph = phase[t];
+            const uint32_t k = ph & 15u;
+            const uint4 pv = __ldg(reinterpret_cast<const uint4*>(
+                a.pat_base[t] + (size_t) k * a.pat_stride[t] + (ph - k)));
+            v.x &= pv.x; v.y &= pv.y; v.z &= pv.z; v.w &= pv.w;
+            uint32_t np = ph + step[t];
+            phase[t] = (np >= a.pat_period[t]) ? np - a.pat_period[t] : np;
+          }
+        }
+        if (c == 0 && segLow <= a.presieve_max) {
+          // The patterns also cleared the pre-sieve primes themselves;
+          // put them back (reference: restore bytes, GpuTables.cpp:108-127).
+          uint32_t w4[4] = { v.x, v.y, v.z, v.w };
+          for (uint32_t i = 0; i < a.num_presieve_primes; i++) {
+            const uint64_t q = a.presieve_primes[i];
+            if (q < segLow + 7) continue;
+            const uint64_t rel = q - segLow - 7;      // < 16*30
+            const uint32_t byte = (uint32_t) (rel / 30u);
+            if (byte >= 16) continue;
+            const uint32_t bit = residue_to_bit((uint32_t) (q % 30u));
+            w4[byte >> 2] |= 1u << (8 * (byte & 3) + bit);
+          }
+          v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+        smem4[c] = v;
+      }
+    }
+    __syncthreads();
+
+    // ---- 2. small primes: one warp per prime ----------------------------
+    {
+      const uint32_t j = lane & 7u;
+      const uint32_t r = lane >> 3;
+      const uint32_t Q = cofactor_class(j);
+      for (uint32_t i = warp; i < a.n_small; i += NWARPS) {
+        const uint32_t p = a.primes[i];
+        const uint64_t rcp = a.recip[i];
+        uint64_t d; uint32_t c0;
+        first_multiple(segLow, p, rcp, d, c0);
+        if (d >= span) continue;
+        const uint32_t pm = p % 30u;
+        const uint32_t k = (Q + 30u - c0) % 30u;
+        const uint64_t off = d + (uint64_t) k * p;          // value offset
+        const uint64_t b64 = off / 30u + (uint64_t) r * p;  // byte index
+        if (b64 < seg_bytes) {
+          const uint32_t b = (uint32_t) b64;
+          const uint32_t bit = residue_to_bit((Q * pm) % 30u);
+          const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
+          for (uint32_t w = b >> 2; w < nwords; w += p)
+            atomicAnd(&sieve32[w], mask);
+        }
+      }
+    }
+
+    // ---- 3. medium primes: one thread per prime --------------------------
+    for (uint32_t i = a.n_small + tid; i < a.n_primes; i += BLOCK) {
+      const uint32_t p = a.primes[i];
+      const uint64_t rcp = a.recip[i];
+      uint64_t d; uint32_t c0;
+      first_multiple(segLow, p, rcp, d, c0);
+      if (d / 30u >= seg_bytes) continue;
+      const uint32_t pm = p % 30u;
+#pragma unroll
+      for (uint32_t j = 0; j < 8; j++) {
+        const uint32_t Q = cofactor_class(j);
+        const uint32_t k = (Q + 30u - c0) % 30u;
+        uint64_t b = (d + (uint64_t) k * p) / 30u;
+        if (b < seg_bytes) {
+          const uint32_t bit = residue_to_bit((Q * pm) % 30u);
+          do {
+            const uint32_t bb = (uint32_t) b;
+            atomicAnd(&sieve32[bb >> 2], ~(1u << (bit + 8u * (bb & 3u))));
+            b += p;
+          } while (b < seg_bytes);
+        }
+      }
+    }
+
+    // ---- 4. big primes: bucket lists of this segment ---------------------
+    if (a.num_bucket_lists) {
+      const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
+      const uint32_t* seg_entries = a.bucket_entries + s * a.bucket_seg_stride;
+      for (uint32_t l = warp; l < a.num_bucket_lists; l += NWARPS) {
+        const uint32_t n = cnt[l];
+        const uint32_t* e = seg_entries + a.bucket_list_off[l];
+        for (uint32_t x = lane; x < n; x += 32) {
+          const uint32_t v = __ldg(e + x);
+          // entry: byte index << 3 | bit
+          const uint32_t b = v >> 3;
+          atomicAnd(&sieve32[b >> 2], ~(1u << ((v & 7u) + 8u * (b & 3u))));
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- 5. mask the range edges and count -------------------------------
+    {
+      const uint64_t rhi = a.hi - segLow;                   // >= 7
+      const uint64_t rlo = (a.lo > segLow) ? a.lo - segLow : 0;
+      const bool full = (rlo <= 7) && (rhi >= span + 1);
+      uint32_t c[6] = { 0, 0, 0, 0, 0, 0 };
+      for (uint32_t ch = tid; ch < nchunks; ch += BLOCK) {
+        uint4 v = smem4[ch];
+        if (!full) {
+          uint32_t w4[4] = { v.x, v.y, v.z, v.w };
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            uint32_t m = 0;
+#pragma unroll
+            for (int by = 0; by < 4; by++) {
+              const uint64_t base = 30ull * (16ull * ch + 4u * q + by);
+              m |= byte_keep(base, rlo, rhi) << (8 * by);
+            }
+            w4[q] &= m;
+          }
+          v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+        count_word<ALL_KINDS>(v.x, c);
+        count_word<ALL_KINDS>(v.y, c);
+        count_word<ALL_KINDS>(v.z, c);
+        count_word<ALL_KINDS>(v.w, c);
+      }
+#pragma unroll
+      for (int k = 0; k < 6; k++) acc[k] += c[k];
+    }
+    __syncthreads();
+  }
+
+  // ---- warp reduction, one atomic per warp and kind ----------------------
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    if (!ALL_KINDS && k > 0) break;
+    uint64_t v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && v && ((a.kinds >> k) & 1u))
+      atomicAdd(&a.counts[k], (unsigned long long) v);
+  }
+}
+
+} // namespace psg
