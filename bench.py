@@ -1,0 +1,351 @@
+#!/usr/bin/env python3
+"""Benchmark: integers sieved per second, exact prime counts, on B200.
+
+Workload (one step = one full pass): count the primes in
+[1e15, 1e15 + 1e11] -- 1,951,957 sieving primes up to ~3.16e7, so the bucket
+sieve (big primes) and the shared-memory cross-off (small and medium primes)
+both run. With N GPUs (one process per GPU under torchrun) rank r counts
+[1e15 + r*1e11, 1e15 + (r+1)*1e11] (weak scaling) and the totals are summed
+with one NCCL all_reduce.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value : device-timed throughput (CUDA events on the launch stream around K
+        passes of psg_count_async; the sieving-prime table is prepared in the
+        warm-up, so the timed region is pure GPU work), max over ranks.
+e2e   : the same metric through the C ABI call psg_count() with host
+        arguments and a host result (launches, accumulator reset and the
+        device->host copy inside the timed region), wall clock, max over ranks.
+--impl reference : the reference's own CPU sieve (oracle/_ref/primesieve,
+        built from the reference sources) on all host cores, on bounded
+        samples of the same workload; the C restatement in oracle/ stands in
+        if that binary is missing.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+START = 10 ** 15
+LENGTH = 10 ** 11
+METRIC = "integers sieved/s, exact pi/k-tuplet counts: batched vs per-range; p50/p99 latency"
+UNIT = "integers/s"
+WORKLOAD = "count primes in [1e15, 1e15+1e11] (sieving primes <= 3.16e7, bucket sieve)"
+GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def load_pkg():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("primesieve_gpu_b200",
+                                                  os.path.join(REPO, "primesieve-gpu_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"psg_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_reference_rate(budget_s, threads=None):
+    """The reference's CPU sieve on this host: largest sample of the workload
+    [1e15, 1e15+S] that takes about `budget_s` seconds. Returns
+    (integers/s, sample length, seconds, kind, cores)."""
+    exe = os.path.join(REPO, "oracle", "_ref", "primesieve")
+    cores = threads or os.cpu_count() or 1
+    if os.path.exists(exe):
+        def run(n):
+            t = time.perf_counter()
+            out = subprocess.run([exe, str(START), str(START + n), "-c1", "-q", "-t", str(cores)],
+                                 capture_output=True, text=True, check=True).stdout
+            return time.perf_counter() - t, int(out.split()[0])
+        kind = "reference"
+    else:
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        from conftest import Oracle  # the C restatement (single-threaded), checker only
+        orc = Oracle()
+        cores = 1
+
+        def run(n):
+            t = time.perf_counter()
+            c = orc.plain(START, START + n, 1)[0]
+            return time.perf_counter() - t, c
+        kind = "port"
+    n = 10 ** 9
+    el, _ = run(n)
+    while el < budget_s / 4 and n < LENGTH:
+        n = min(LENGTH, int(n * max(2.0, min(8.0, budget_s / max(el, 1e-3) / 2))))
+        el, _ = run(n)
+    return n / el, n, el, kind, cores
+
+
+def reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    # per step: one bounded sample of the workload sized to ~6 s of CPU work
+    rate, n, el, kind, cores = cpu_reference_rate(6.0)
+    exe = os.path.join(REPO, "oracle", "_ref", "primesieve")
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        if kind == "reference":
+            subprocess.run([exe, str(START), str(START + n), "-c1", "-q", "-t", str(cores)],
+                           capture_output=True, check=True)
+        else:
+            sys.path.insert(0, os.path.join(REPO, "tests"))
+            from conftest import Oracle
+            Oracle().plain(START, START + n, 1)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t)
+    total = sum(times)
+    value = n * len(times) / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sample": f"[1e15, 1e15+{n:.3g}] per step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"[1e15, 1e15+{n:.3g}] per step, -t {cores}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+    import torch.distributed as dist
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    psg = load_pkg()
+    ctx = psg.Context(device=local)
+    a = START + rank * LENGTH
+    b = a + LENGTH
+    # a dedicated (non-default) stream: the kernels, the accumulator reset and
+    # the CUDA events all go on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    counts = torch.zeros(6, dtype=torch.int64, device="cuda")
+    ctx.prepare(b)
+
+    def step():
+        counts.zero_()
+        ctx.count_async(a, b, psg.PRIMES, counts.data_ptr(), stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    got0 = int(counts[0].item())
+
+    # ---- device-timed region ------------------------------------------------
+    ctx.reset_kernel_stats()
+    ctx.bucket_entries(reset=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    stats = ctx.kernel_stats()
+    launches = sum(v[0] for v in stats.values())
+    entries = ctx.bucket_entries(reset=True)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * LENGTH * args.steps / (ms_max * 1e-3)
+
+    # ---- per-kernel roofline (CUDA events per launch, separate pass) --------
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    step()
+    torch.cuda.synchronize()
+    kst = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    smem_rate = ctx.smem_atomic_rate()
+    hbm_peak, peak_src = load_peaks()
+    entries_per_pass = entries / args.steps
+    sieve_l, sieve_ms = kst.get("sieve_count_kernel", (0, 0.0))
+    fill_l, fill_ms = kst.get("bucket_fill_kernel", (0, 0.0))
+    # algorithmic bytes of the bucket kernel: 4 B per entry written
+    fill_bytes = 4.0 * entries_per_pass
+    fill_gbs = fill_bytes / max(fill_ms, 1e-9) / 1e6
+    # cross-off phase: crossings = (8/30) * N * sum(1/p) over sieving primes
+    # p > 59 (pre-sieved below); the sieve kernel does these with shared atomics
+    crossings = crossing_count(b)
+    sieve_rate = crossings / max(sieve_ms * 1e-3, 1e-12)
+    dominant = "bucket_fill_kernel" if fill_ms > sieve_ms else "sieve_count_kernel"
+    roof_fill = {"kernel": "bucket_fill_kernel", "bound": "hbm", "achieved": fill_gbs, "peak": hbm_peak,
+                 "unit": "GB/s", "frac": fill_gbs / hbm_peak, "traffic": None,
+                 "algorithmic_bytes_per_launch": fill_bytes / max(fill_l, 1),
+                 "avg_launch_ms": fill_ms / max(fill_l, 1), "peak_source": peak_src}
+    roof_sieve = {"kernel": "sieve_count_kernel", "bound": "smem_atomic", "achieved": sieve_rate / 1e9,
+                  "peak": smem_rate / 1e9, "unit": "Gatomic/s", "frac": sieve_rate / max(smem_rate, 1),
+                  "traffic": None, "crossings_per_pass": crossings,
+                  "bucket_entries_applied_per_pass": entries_per_pass,
+                  "avg_launch_ms": sieve_ms / max(sieve_l, 1),
+                  "peak_source": "measured in-run (random-address smem atomicAnd probe)"}
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    # psg_count: host arguments in, host counts out (launches, the device
+    # accumulator reset and the device->host copy all inside the timed region)
+    ctx.count(a, b, psg.PRIMES)
+    barrier()
+    te = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        e2e_count = ctx.count(a, b, psg.PRIMES)[0]
+    te = time.perf_counter() - te
+    te_t = torch.tensor([te], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * LENGTH * max(1, args.steps // 2) / float(te_t.item())
+
+    tot = torch.tensor([got0], dtype=torch.int64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ok0 = (rank != 0) or (got0 == GOLDEN_1E15 and e2e_count == GOLDEN_1E15)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, n, el, kind, cores = cpu_reference_rate(12.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"[1e15, 1e15+{n:.3g}] in {el:.1f} s, -t {cores}"}
+
+    if rank == 0:
+        cfg = ctx.config()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "range_per_gpu": [a, b], "kinds": "primes",
+                       "segment_bytes": cfg["seg_bytes"], "block": cfg["block"],
+                       "l2": "inputs larger than L2: each pass streams %.1f GB of bucket lists" % (8 * entries_per_pass / 1e9),
+                       "count_ok": bool(ok0), "total_count": int(tot.item())},
+            "roofline": roof_fill if dominant == "bucket_fill_kernel" else roof_sieve,
+            "rooflines": [roof_sieve, roof_fill],
+            "kernel_ms_per_pass": {k: v[1] for k, v in kst.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 16, "d2h_bytes_per_step": 52,
+                    "api": "psg_count (C ABI, host result)"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0 if ok0 else 1
+
+
+def crossing_count(stop):
+    """Crossings of one pass: sum over sieving primes 59 < p <= sqrt(stop) of
+    the multiples p*q (q coprime to 30) in the range, (8/30) * LENGTH / p."""
+    import math
+    import numpy as np
+    lim = math.isqrt(stop)
+    sieve = np.ones(lim + 1, dtype=bool)
+    sieve[:2] = False
+    for i in range(2, math.isqrt(lim) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = False
+    p = np.nonzero(sieve)[0]
+    p = p[p > 59].astype(np.float64)
+    return float(LENGTH * 8.0 / 30.0 * np.sum(1.0 / p))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,62 @@
+/*
+ * primesieve.h -- primesieve-compatible C API of the B200 counting engine.
+ *
+ * Drop-in for the counting subset of the reference's C API
+ * (include/primesieve.h:130-233, implementation src/api-c.cpp:143-225).
+ * Every count runs on the GPU (no CPU fallback, no minimum range). On error
+ * the functions print a message to stderr, set errno to EDOM and return
+ * PRIMESIEVE_ERROR, exactly like the reference.
+ *
+ * The reference's prime generation, printing and nth-prime functions are not
+ * part of this library (counting path only).
+ */
+#ifndef PRIMESIEVE_H
+#define PRIMESIEVE_H
+
+#define PRIMESIEVE_VERSION "12.16"
+#define PRIMESIEVE_VERSION_MAJOR 12
+#define PRIMESIEVE_VERSION_MINOR 16
+
+#include <stddef.h>
+#include <stdint.h>
+
+/* Returned by the uint64_t functions on error (reference include/primesieve.h:31). */
+#define PRIMESIEVE_ERROR ((uint64_t) ~((uint64_t) 0))
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Count the primes / prime k-tuplets inside [start, stop], stop <= 2^64-1.
+ * Reference: include/primesieve.h:130-170, src/api-c.cpp:143-225. */
+uint64_t primesieve_count_primes(uint64_t start, uint64_t stop);
+uint64_t primesieve_count_twins(uint64_t start, uint64_t stop);
+uint64_t primesieve_count_triplets(uint64_t start, uint64_t stop);
+uint64_t primesieve_count_quadruplets(uint64_t start, uint64_t stop);
+uint64_t primesieve_count_quintuplets(uint64_t start, uint64_t stop);
+uint64_t primesieve_count_sextuplets(uint64_t start, uint64_t stop);
+
+/* All six counts of [start, stop] from one sieve pass (no reference
+ * counterpart: the reference counts one kind per GPU pass,
+ * src/app/main.cpp:158-160). counts[i] = primes, twins, ..., sextuplets.
+ * Returns 0, or -1 on error (message on stderr, errno = EDOM). */
+int primesieve_count_all(uint64_t start, uint64_t stop, uint64_t counts[6]);
+
+/* 2^64-1 (reference src/api.cpp:169-172). */
+uint64_t primesieve_get_max_stop(void);
+
+/* CPU tuning knobs of the reference (include/primesieve.h:205-233). They are
+ * accepted and reported back but do not influence the GPU sieve. */
+int primesieve_get_sieve_size(void);
+int primesieve_get_num_threads(void);
+void primesieve_set_sieve_size(int sieve_size);
+void primesieve_set_num_threads(int num_threads);
+
+/* "12.16" (the API version this library implements). */
+const char* primesieve_version(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif

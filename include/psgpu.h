@@ -67,8 +67,9 @@ typedef struct {
   uint32_t big_limit;          /* sieving primes from: bucket sieve */
   uint32_t window_segments;    /* segments per bucket window */
   uint32_t bucket_lists;       /* bucket lists per segment */
-  uint32_t presieve;           /* 1 = pre-sieve with pattern tables (default) */
+  uint32_t presieve;           /* pre-sieve with pattern tables: 0 = default (on), 1 = on, 2 = off */
   uint32_t segments_per_launch;/* cap on segments per launch (reference knob) */
+  uint32_t sweep_limit;        /* big primes below: segment-major bucket sweep */
 } psg_config;
 
 /* A [start, stop] range and the kinds wanted for it (batch API). */
@@ -124,6 +125,12 @@ int psg_set_profiling(psg_context* ctx, int on);
 int psg_kernel_stats(psg_context* ctx, const char** names, uint64_t* launches,
                      double* ms, size_t cap, size_t* n);
 int psg_reset_kernel_stats(psg_context* ctx);
+/* Bucket-sieve entries written (4 bytes each) since the last reset; waits for
+ * the context's stream. reset != 0 zeroes the counter afterwards. */
+int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset);
+/* Roofline denominator of the cross-off phase: the measured rate of
+ * random-address shared-memory atomicAnd on this device (atomics/s). */
+int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s);
 
 /* The library version string. */
 const char* psg_version(void);

@@ -27,6 +27,7 @@ PSG_SYMBOLS = (
     "psg_get_config", "psg_describe", "psg_count", "psg_count_async",
     "psg_count_batch", "psg_prepare", "psg_last_error", "psg_status_string",
     "psg_set_profiling", "psg_kernel_stats", "psg_reset_kernel_stats", "psg_version",
+    "psg_bucket_entries", "psg_measure_smem_atomic_rate",
 )
 
 
@@ -41,7 +42,7 @@ class PsgError(RuntimeError):
 class PsgConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in (
         "seg_bytes", "block", "ctas_per_sm", "small_limit", "big_limit",
-        "window_segments", "bucket_lists", "presieve", "segments_per_launch")]
+        "window_segments", "bucket_lists", "presieve", "segments_per_launch", "sweep_limit")]
 
 
 class PsgRange(ctypes.Structure):
@@ -81,6 +82,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_kernel_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_char_p), U64P,
                                      ctypes.POINTER(ctypes.c_double), sz, ctypes.POINTER(sz)]
     lib.psg_reset_kernel_stats.argtypes = [vp]
+    lib.psg_bucket_entries.argtypes = [vp, U64P, i32]
+    lib.psg_measure_smem_atomic_rate.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.psg_version.restype = ctypes.c_char_p
     for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
         fn = getattr(lib, "primesieve_count_" + name, None)
@@ -185,6 +188,16 @@ class Context:
     def reset_kernel_stats(self) -> None:
         _check(self._lib.psg_reset_kernel_stats(self._h))
 
+    def smem_atomic_rate(self) -> float:
+        v = ctypes.c_double(0)
+        _check(self._lib.psg_measure_smem_atomic_rate(self._h, ctypes.byref(v)))
+        return v.value
+
+    def bucket_entries(self, reset: bool = False) -> int:
+        v = ctypes.c_uint64(0)
+        _check(self._lib.psg_bucket_entries(self._h, ctypes.byref(v), 1 if reset else 0))
+        return v.value
+
 
 def split_range(start: int, stop: int, parts: int) -> List[Tuple[int, int]]:
     """Split [start, stop] into `parts` consecutive sub-ranges whose inner
@@ -202,3 +215,32 @@ def split_range(start: int, stop: int, parts: int) -> List[Tuple[int, int]]:
         bounds.append(max(b, bounds[-1]))
     bounds.append(stop + 1)
     return [(a, b - 1) for a, b in zip(bounds, bounds[1:]) if a <= b - 1]
+
+
+def shard_of(start: int, stop: int, rank: int, world: int) -> Optional[Tuple[int, int]]:
+    """This rank's part of [start, stop] for a one-process-per-GPU run: the
+    range is cut into `world` consecutive parts at == 2 (mod 30) boundaries
+    (no collective is needed to count them; only the six totals are summed)."""
+    parts = split_range(start, stop, world)
+    # split_range drops empty parts; re-split so that rank indices line up
+    if len(parts) < world:
+        parts = parts + [None] * (world - len(parts))
+    return parts[rank]
+
+
+def count_sharded(count_fn, start: int, stop: int, kinds: int, rank: int, world: int,
+                  group=None) -> List[int]:
+    """Count [start, stop] across `world` ranks: each rank counts its shard
+    with count_fn(a, b, kinds) -> [6 counts], then the six totals are summed
+    with one all_reduce over torch.distributed (NCCL on GPUs, gloo on CPU)."""
+    import torch
+    import torch.distributed as dist
+    part = shard_of(start, stop, rank, world)
+    local = count_fn(part[0], part[1], kinds) if part else [0] * 6
+    if world == 1 or not dist.is_initialized():
+        return list(local)
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    t = torch.tensor([int(x) for x in local], dtype=torch.int64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return [int(x) for x in t.cpu().tolist()]

@@ -40,6 +40,7 @@ psg::EngineConfig to_engine(const psg_config* c) {
   e.bucket_lists = c->bucket_lists;
   e.presieve = c->presieve;
   e.segments_per_launch = c->segments_per_launch;
+  e.sweep_limit = c->sweep_limit;
   return e;
 }
 
@@ -125,6 +126,7 @@ int psg_get_config(const psg_context* ctx, psg_config* out) {
   out->bucket_lists = c.bucket_lists;
   out->presieve = c.presieve;
   out->segments_per_launch = c.segments_per_launch;
+  out->sweep_limit = c.sweep_limit;
   return PSG_OK;
 }
 
@@ -190,6 +192,21 @@ int psg_kernel_stats(psg_context* ctx, const char** names, uint64_t* launches, d
     if (ms) ms[i] = st[i].ms;
   }
   return PSG_OK;
+}
+
+int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset) {
+  if (!ctx || !total) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  *total = ctx->engine.bucket_entries();
+  if (reset) ctx->engine.reset_bucket_entries();
+  return PSG_OK;
+}
+
+int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s) {
+  if (!ctx || !atomics_per_s) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  *atomics_per_s = ctx->engine.measure_smem_atomic_rate();
+  return *atomics_per_s > 0 ? PSG_OK : fail(PSG_ERR_CUDA, "probe kernel failed");
 }
 
 int psg_reset_kernel_stats(psg_context* ctx) {

@@ -2,6 +2,7 @@
 #include "engine.hpp"
 #include "sieve_kernel.cuh"
 #include "bucket_kernel.cuh"
+#include "sweep_kernel.cuh"
 #include "../../include/psgpu.h"
 
 #include <algorithm>
@@ -12,6 +13,10 @@
 namespace psg {
 
 namespace {
+
+constexpr int kBucketBlock = 1024;
+constexpr int kSweepWarps = 16;     // sweep CTA = 512 threads
+constexpr int kSweepK = 16;         // sieving primes per sweep lane
 
 #define PSG_CUDA(call)                                                          \
   do {                                                                          \
@@ -126,7 +131,49 @@ cudaError_t launch_sieve(uint32_t block, bool all, uint32_t grid, uint32_t smem,
   return cudaGetLastError();
 }
 
+// Roofline probe: random-address shared-memory atomicAnd throughput (the
+// operation the cross-off phase is made of). Each thread walks its own odd
+// word stride through a 32 KiB shared array; indices stay below kProbeWords.
+constexpr uint32_t kProbeWords = 8192;    // 32 KiB of static shared memory
+__global__ void __launch_bounds__(512) smem_atomic_probe_kernel(uint32_t iters, uint32_t* out) {
+  __shared__ uint32_t s[kProbeWords];
+  for (uint32_t i = threadIdx.x; i < kProbeWords; i += blockDim.x) s[i] = ~0u;
+  __syncthreads();
+  uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u;
+  h ^= h >> 15; h *= 0x2c1b3c6du; h ^= h >> 12;
+  uint32_t w = h % kProbeWords;
+  const uint32_t stride = 2u * ((h >> 8) % 2048u) + 1u;     // < kProbeWords
+  for (uint32_t it = 0; it < iters; it++) {
+    atomicAnd(&s[w], ~(1u << (it & 31u)));
+    w += stride;
+    if (w >= kProbeWords) w -= kProbeWords;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) out[blockIdx.x] = s[0];
+}
+
 } // namespace
+
+double Engine::measure_smem_atomic_rate() {
+  cudaSetDevice(device_);
+  const int grid = prop_.multiProcessorCount * 2;
+  uint32_t* out = nullptr;
+  if (cudaMalloc(&out, grid * sizeof(uint32_t)) != cudaSuccess) { cudaGetLastError(); return 0; }
+  cudaEvent_t a, b;
+  cudaEventCreate(&a); cudaEventCreate(&b);
+  smem_atomic_probe_kernel<<<grid, 512, 0, stream_>>>(64, out);
+  const uint32_t iters = 8192;
+  cudaEventRecord(a, stream_);
+  smem_atomic_probe_kernel<<<grid, 512, 0, stream_>>>(iters, out);
+  cudaEventRecord(b, stream_);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a); cudaEventDestroy(b);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0) return 0;
+  return (double) grid * 512.0 * iters / (ms * 1e-3);
+}
 
 Engine::~Engine() {
   if (device_ < 0) return;
@@ -141,9 +188,14 @@ Engine::~Engine() {
   cudaFree(d_bcounts_);
   cudaFree(d_list_off_);
   cudaFree(d_list_cap_);
+  cudaFree(d_chunk_begin_);
+  cudaFree(d_sweep_b_);
+  cudaFree(d_sweep_i_);
   cudaFree(d_overflow_);
+  cudaFree(d_entry_total_);
   cudaFree(d_counts_);
   if (h_counts_) cudaFreeHost(h_counts_);
+  if (done_event_) cudaEventDestroy(done_event_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -177,51 +229,75 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
     return PSG_ERR_NO_DEVICE;
   }
   PSG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  PSG_CUDA(cudaEventCreateWithFlags(&done_event_, cudaEventDisableTiming));
 
   // ---- geometry ------------------------------------------------------------
-  block_ = cfg.block ? cfg.block : 512;
+  // Shared memory per CTA = sieve segment + medium-prime state. By default
+  // one 1024-thread CTA per SM holds a 128 KiB segment and gives the rest of
+  // the SM's shared memory to the carried medium-prime state.
+  block_ = cfg.block ? cfg.block : 1024;
   if (block_ != 256 && block_ != 512 && block_ != 1024) {
     err = "block must be 256, 512 or 1024";
     return PSG_ERR_ARG;
   }
+  const uint32_t target_ctas = cfg.ctas_per_sm ? cfg.ctas_per_sm : 1;
   const uint32_t smem_optin = (uint32_t) prop_.sharedMemPerBlockOptin;
-  seg_bytes_ = cfg.seg_bytes ? cfg.seg_bytes : 65536u;
-  seg_bytes_ = std::min(seg_bytes_, smem_optin);
+  const uint32_t smem_sm = (uint32_t) prop_.sharedMemPerMultiprocessor;
+  uint32_t budget = smem_sm / target_ctas;
+  budget = (budget > 1024u + 128u) ? budget - 1024u - 128u : 0u;   // driver reserve + static smem
+  budget = std::min(budget, smem_optin - 128u) & ~15u;
+  seg_bytes_ = cfg.seg_bytes ? cfg.seg_bytes : 131072u;
+  seg_bytes_ = std::min(seg_bytes_, budget);
   seg_bytes_ &= ~(16u * block_ - 1u);          // whole 16-byte chunks per thread
   if (seg_bytes_ < 16u * block_) {
     err = "segment too small for the block size";
     return PSG_ERR_ARG;
   }
+  state_cap_ = (budget - seg_bytes_) / 4u;
+  smem_dyn_ = seg_bytes_ + 4u * state_cap_;
   switch (block_) {
-    case 256: set_smem_attrs<256>(seg_bytes_); break;
-    case 1024: set_smem_attrs<1024>(seg_bytes_); break;
-    default: set_smem_attrs<512>(seg_bytes_); break;
+    case 256: set_smem_attrs<256>(smem_dyn_); break;
+    case 1024: set_smem_attrs<1024>(smem_dyn_); break;
+    default: set_smem_attrs<512>(smem_dyn_); break;
   }
-  int occ = block_ == 256 ? occupancy<256>(seg_bytes_)
-          : block_ == 1024 ? occupancy<1024>(seg_bytes_) : occupancy<512>(seg_bytes_);
+  int occ = block_ == 256 ? occupancy<256>(smem_dyn_)
+          : block_ == 1024 ? occupancy<1024>(smem_dyn_) : occupancy<512>(smem_dyn_);
   if (occ < 1) {
     err = "sieve kernel cannot be resident with this segment/block size";
     return PSG_ERR_ARG;
   }
-  if (cfg.ctas_per_sm) occ = std::min<int>(occ, (int) cfg.ctas_per_sm);
+  occ = std::min<int>(occ, (int) target_ctas);
   grid_ = (uint32_t) (prop_.multiProcessorCount * occ);
 
   const uint64_t span = (uint64_t) seg_bytes_ * 30u;
-  small_limit_ = cfg.small_limit ? cfg.small_limit : seg_bytes_ / 8u;
+  small_limit_ = cfg.small_limit ? cfg.small_limit : 4096u;
   big_limit_ = cfg.big_limit ? cfg.big_limit : (uint32_t) std::min<uint64_t>(span / 10u, 0xffffffffull);
   if (big_limit_ < small_limit_) big_limit_ = small_limit_;
   window_ = cfg.window_segments ? cfg.window_segments : grid_ * 4u;
-  window_ = std::min<uint32_t>(window_, 12000u);     // counters must fit in smem
-  lists_ = cfg.bucket_lists ? cfg.bucket_lists : (uint32_t) prop_.multiProcessorCount * 2u;
-  cudaFuncSetAttribute(bucket_fill_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) (window_ * sizeof(uint32_t)));
+  // the bucket fill kernel scans W <= 8 * its block size segment counters
+  // and packs (segment, byte << 3 | bit) into 32 bits
+  entry_bits_ = 3;
+  while ((1u << (entry_bits_ - 3)) < seg_bytes_) entry_bits_++;
+  window_ = std::min<uint32_t>(window_, std::min<uint32_t>(8u * kBucketBlock, 1u << (32 - entry_bits_)));
+  lists_ = cfg.bucket_lists ? cfg.bucket_lists : (uint32_t) prop_.multiProcessorCount;
+  // the bucket kernel indexes a window with 32-bit byte offsets
+  window_ = std::min<uint32_t>(window_, (uint32_t) ((1ull << 31) / seg_bytes_));
+  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) fill_smem_bytes<kBucketBlock>(window_));
+  cudaFuncSetAttribute(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (window_ * sizeof(uint32_t)));
+  // sweep primes need pdiv30 < 2^22 (state packing): p < 1.25e8
+  // (default: off -- the staged prime-major fill is faster on B200)
+  sweep_limit_ = std::min<uint32_t>(cfg.sweep_limit, 120000000u);
 
   PSG_CUDA(cudaMalloc(&d_counts_, 6 * sizeof(unsigned long long)));
   PSG_CUDA(cudaMalloc(&d_overflow_, sizeof(uint32_t)));
+  PSG_CUDA(cudaMalloc(&d_entry_total_, sizeof(unsigned long long)));
+  PSG_CUDA(cudaMemset(d_entry_total_, 0, sizeof(unsigned long long)));
   PSG_CUDA(cudaMemset(d_overflow_, 0, sizeof(uint32_t)));
   PSG_CUDA(cudaMallocHost(&h_counts_, 8 * sizeof(unsigned long long)));
 
-  if (cfg.presieve == 0) {
+  if (cfg.presieve == 2) {          // 0 = default (on), 1 = on, 2 = off
     presieve_max_ = 5;
   } else {
     int rc = build_presieve(err);
@@ -315,29 +391,70 @@ int Engine::prepare(uint64_t stop, std::string& err) {
   return ensure_primes(std::max<uint32_t>(isqrt64(stop), 7u), err);
 }
 
-// Bucket lists for big primes primes[first, last): one list per bucket CTA
-// (a contiguous chunk of primes), capacity = expected entries per segment
-// + 6 sigma + 32, all lists of one segment packed in one region.
-int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
-  if (first == bucket_first_ && last == bucket_last_ && d_entries_) return PSG_OK;
-  const uint32_t nbig = last - first;
-  const uint32_t lists = std::min<uint32_t>(lists_, nbig);
-  const uint32_t ppl = (nbig + lists - 1) / lists;
+// Bucket lists for the big primes primes[first, last):
+//  * sweep primes [first, mid): the segment-major sweep kernel, one list per
+//    sweep CTA; every CTA holds an interleaved share of the primes, so all
+//    sweep lists get the same capacity (the largest expected count + margin);
+//  * fill primes [mid, last): the prime-major kernel, one list per fill CTA,
+//    chunks cut for equal expected work (setup + hits per window).
+// Capacity = expected entries per segment + 6 sigma + 32 (x cap_scale_
+// after an overflow). All lists of one segment are packed in one region.
+int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::string& err) {
+  if (first == bucket_first_ && mid == bucket_mid_ && last == bucket_last_ && d_entries_) return PSG_OK;
   const double span = (double) seg_bytes_ * 30.0;
-  std::vector<uint32_t> off(lists), cap(lists);
+  const double per_seg = span * (8.0 / 30.0);
+  std::vector<uint32_t> off, cap, begin;
   uint64_t stride = 0;
-  for (uint32_t l = 0; l < lists; l++) {
-    double mu = 0;
-    const uint32_t a = first + l * ppl, b = std::min<uint32_t>(last, a + ppl);
-    for (uint32_t i = a; i < b; i++) mu += span * (8.0 / 30.0) / (double) h_primes_[i];
-    double c = (mu + 6.0 * std::sqrt(mu) + 32.0) * cap_scale_;
-    uint32_t ci = (uint32_t) std::ceil(c);
+  auto add_list = [&](double mu) {
+    uint32_t ci = (uint32_t) std::ceil((mu + 6.0 * std::sqrt(mu) + 32.0) * cap_scale_);
     ci = (ci + 3u) & ~3u;
-    off[l] = (uint32_t) stride;
-    cap[l] = ci;
+    off.push_back((uint32_t) stride);
+    cap.push_back(ci);
     stride += ci;
+  };
+
+  // ---- sweep lists
+  const uint32_t nsweep = mid - first;
+  uint32_t sweep_ctas = 0;
+  if (nsweep) {
+    const uint32_t nw = (nsweep + 32u * kSweepK - 1) / (32u * kSweepK);
+    sweep_ctas = (nw + kSweepWarps - 1) / kSweepWarps;
+    const uint32_t nw_launch = sweep_ctas * kSweepWarps;
+    std::vector<double> mu(sweep_ctas, 0.0);
+    for (uint32_t idx = 0; idx < nsweep; idx++) {
+      const uint32_t gw = (idx / 32u) % nw_launch;
+      mu[gw / kSweepWarps] += per_seg / (double) h_primes_[first + idx];
+    }
+    const double mu_max = *std::max_element(mu.begin(), mu.end());
+    for (uint32_t c = 0; c < sweep_ctas; c++) add_list(mu_max);
   }
+
+  // ---- fill lists
+  const uint32_t nfill = last - mid;
+  uint32_t fill_ctas = 0;
+  if (nfill) {
+    fill_ctas = std::max<uint32_t>(1, std::min<uint32_t>(lists_, nfill));
+    const double win_span = span * (double) window_;
+    const double setup = 8.0;
+    double total = 0;
+    for (uint32_t i = mid; i < last; i++) total += setup + win_span * (8.0 / 30.0) / (double) h_primes_[i];
+    begin.assign(fill_ctas + 1, last);
+    begin[0] = mid;
+    double acc = 0;
+    uint32_t l = 1;
+    for (uint32_t i = mid; i < last && l < fill_ctas; i++) {
+      acc += setup + win_span * (8.0 / 30.0) / (double) h_primes_[i];
+      if (acc >= total * (double) l / (double) fill_ctas) begin[l++] = i + 1;
+    }
+    for (uint32_t c = 0; c < fill_ctas; c++) {
+      double mu = 0;
+      for (uint32_t i = begin[c]; i < begin[c + 1]; i++) mu += per_seg / (double) h_primes_[i];
+      add_list(mu);
+    }
+  }
+  const uint32_t lists = sweep_ctas + fill_ctas;
   if (stride > 0xffffffffull) { err = "bucket region too large"; return PSG_ERR_LIMIT; }
+
   const size_t need_entries = (size_t) stride * window_;
   if (need_entries > entries_cap_) {
     cudaFree(d_entries_); d_entries_ = nullptr; entries_cap_ = 0;
@@ -354,24 +471,37 @@ int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
     PSG_CUDA(cudaMalloc(&d_bcounts_, need_counts * sizeof(uint32_t)));
     bcounts_cap_ = need_counts;
   }
-  if (lists > lists_cap_) {
-    cudaFree(d_list_off_); cudaFree(d_list_cap_);
-    PSG_CUDA(cudaMalloc(&d_list_off_, lists * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&d_list_cap_, lists * sizeof(uint32_t)));
-    lists_cap_ = lists;
+  if (lists + 1 > lists_cap_) {
+    cudaFree(d_list_off_); cudaFree(d_list_cap_); cudaFree(d_chunk_begin_);
+    PSG_CUDA(cudaMalloc(&d_list_off_, (lists + 1) * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&d_list_cap_, (lists + 1) * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&d_chunk_begin_, (lists + 1) * sizeof(uint32_t)));
+    lists_cap_ = lists + 1;
+  }
+  if (nsweep > sweep_state_cap_) {
+    cudaFree(d_sweep_b_); cudaFree(d_sweep_i_);
+    PSG_CUDA(cudaMalloc(&d_sweep_b_, (size_t) nsweep * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&d_sweep_i_, (size_t) nsweep * sizeof(uint32_t)));
+    sweep_state_cap_ = nsweep;
   }
   PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+  if (fill_ctas)
+    PSG_CUDA(cudaMemcpyAsync(d_chunk_begin_, begin.data(), (fill_ctas + 1) * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, stream_));
   PSG_CUDA(cudaStreamSynchronize(stream_));
   seg_stride_ = stride;
   bucket_first_ = first;
+  bucket_mid_ = mid;
   bucket_last_ = last;
-  primes_per_list_ = ppl;
   active_lists_ = lists;
+  sweep_ctas_ = sweep_ctas;
+  fill_ctas_ = fill_ctas;
   return PSG_OK;
 }
 
 void Engine::timed_begin(int which, cudaStream_t st) {
+  timed_[which].launches++;
   if (!profiling_) return;
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
@@ -393,7 +523,6 @@ std::vector<KernelStat> Engine::kernel_stats() {
       float ms = 0;
       cudaEventElapsedTime(&ms, e.first, e.second);
       t.ms += ms;
-      t.launches++;
       cudaEventDestroy(e.first); cudaEventDestroy(e.second);
     }
     t.ev.clear();
@@ -427,10 +556,13 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
   };
   const uint32_t n_total = upto(sq);
   const uint32_t n_small = std::min(below(small_limit_), n_total);
-  const uint32_t n_med = std::min(below(big_limit_), n_total);
+  // medium primes must fit the shared-memory state area; the rest go to buckets
+  const uint32_t n_med = std::max(n_small, std::min({ below(big_limit_), n_total, n_small + state_cap_ }));
   const bool use_buckets = n_med < n_total;
+  // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
+  const uint32_t n_sweep_end = std::max(n_med, std::min(below(sweep_limit_), n_total));
   if (use_buckets) {
-    rc = ensure_buckets(n_med, n_total, err);
+    rc = ensure_buckets(n_med, n_sweep_end, n_total, err);
     if (rc) return rc;
   }
 
@@ -453,6 +585,10 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
   a.recip = d_recip_;
   a.n_small = n_small;
   a.n_primes = n_med;
+  for (uint32_t c = 0; c < 8; c++) {
+    a.wheel_tab[2 * c] = wheel_bits_packed(c);
+    a.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
+  }
   a.kinds = kinds;
   a.counts = dev_counts;
   const bool all = (kinds & ~1u) != 0;
@@ -465,28 +601,64 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
     a.seg_low0 = win_low;
     a.num_segments = ns;
     if (use_buckets) {
-      BucketArgs b;
-      std::memset(&b, 0, sizeof b);
-      b.win_low = win_low;
-      b.win_segments = (uint32_t) ns;
-      b.seg_bytes = seg_bytes_;
-      b.seg_rcp = 0xffffffffffffffffull / seg_bytes_;
-      b.primes = d_primes_;
-      b.recip = d_recip_;
-      b.first = bucket_first_;
-      b.last = bucket_last_;
-      b.primes_per_list = primes_per_list_;
-      b.num_lists = active_lists_;
-      b.list_off = d_list_off_;
-      b.list_cap = d_list_cap_;
-      b.seg_stride = seg_stride_;
-      b.entries = d_entries_;
-      b.counts = d_bcounts_;
-      b.overflow = d_overflow_;
-      timed_begin(1, st);
-      bucket_fill_kernel<256><<<active_lists_, 256, (size_t) ns * sizeof(uint32_t), st>>>(b);
-      timed_end(1, st);
-      PSG_CUDA(cudaGetLastError());
+      if (sweep_ctas_) {
+        SweepArgs w;
+        std::memset(&w, 0, sizeof w);
+        w.win_low = win_low;
+        w.win_segments = (uint32_t) ns;
+        w.seg_bytes = seg_bytes_;
+        w.primes = d_primes_;
+        w.recip = d_recip_;
+        w.first = bucket_first_;
+        w.n = bucket_mid_ - bucket_first_;
+        w.init = (s0 == 0) ? 1u : 0u;
+        w.state_b = d_sweep_b_;
+        w.state_i = d_sweep_i_;
+        w.list_base = 0;
+        w.num_lists_total = active_lists_;
+        w.list_off = d_list_off_;
+        w.list_cap = d_list_cap_;
+        w.seg_stride = seg_stride_;
+        w.entries = d_entries_;
+        w.counts = d_bcounts_;
+        w.overflow = d_overflow_;
+        w.entry_total = d_entry_total_;
+        for (uint32_t c = 0; c < 8; c++) {
+          w.wheel_tab[2 * c] = wheel_bits_packed(c);
+          w.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
+        }
+        timed_begin(2, st);
+        bucket_sweep_kernel<32 * kSweepWarps, kSweepK>
+            <<<sweep_ctas_, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), st>>>(w);
+        timed_end(2, st);
+        PSG_CUDA(cudaGetLastError());
+      }
+      if (fill_ctas_) {
+        BucketArgs b;
+        std::memset(&b, 0, sizeof b);
+        b.win_low = win_low;
+        b.win_segments = (uint32_t) ns;
+        b.seg_bytes = seg_bytes_;
+        b.seg_magic = (uint32_t) ((1ull << 32) / seg_bytes_ + 1u);
+        b.entry_bits = entry_bits_;
+        b.primes = d_primes_;
+        b.recip = d_recip_;
+        b.chunk_begin = d_chunk_begin_;
+        b.list_base = sweep_ctas_;
+        b.num_lists = active_lists_;
+        b.list_off = d_list_off_;
+        b.list_cap = d_list_cap_;
+        b.seg_stride = seg_stride_;
+        b.entries = d_entries_;
+        b.counts = d_bcounts_;
+        b.overflow = d_overflow_;
+        b.entry_total = d_entry_total_;
+        timed_begin(1, st);
+        bucket_fill_kernel<kBucketBlock>
+            <<<fill_ctas_, kBucketBlock, fill_smem_bytes<kBucketBlock>((uint32_t) ns), st>>>(b);
+        timed_end(1, st);
+        PSG_CUDA(cudaGetLastError());
+      }
       a.bucket_entries = d_entries_;
       a.bucket_counts = d_bcounts_;
       a.bucket_list_off = d_list_off_;
@@ -495,7 +667,7 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
     }
     const uint32_t g = (uint32_t) std::min<uint64_t>(grid_, ns);
     timed_begin(0, st);
-    cudaError_t e = launch_sieve(block_, all, g, seg_bytes_, st, a);
+    cudaError_t e = launch_sieve(block_, all, g, smem_dyn_, st, a);
     timed_end(0, st);
     if (e != cudaSuccess) {
       err = std::string("sieve kernel launch: ") + cudaGetErrorString(e);
@@ -509,6 +681,18 @@ int Engine::count_async(uint64_t start, uint64_t stop, uint32_t kinds,
                         unsigned long long* dev_counts, cudaStream_t stream, std::string& err) {
   PSG_CUDA(cudaSetDevice(device_));
   cudaStream_t st = stream ? stream : stream_;
+  // The engine's scratch (bucket lists, sweep state) is shared by all counts
+  // of this context: order this count after the previous one, whatever
+  // stream that one ran on.
+  if (last_stream_ && last_stream_ != st) PSG_CUDA(cudaStreamWaitEvent(st, done_event_, 0));
+  int rc = count_enqueue(start, stop, kinds, dev_counts, st, err);
+  PSG_CUDA(cudaEventRecord(done_event_, st));
+  last_stream_ = st;
+  return rc;
+}
+
+int Engine::count_enqueue(uint64_t start, uint64_t stop, uint32_t kinds,
+                          unsigned long long* dev_counts, cudaStream_t st, std::string& err) {
   kinds &= 0x3fu;
   if (start > stop || kinds == 0) return PSG_OK;
   uint64_t tab[6] = { 0, 0, 0, 0, 0, 0 };
@@ -543,10 +727,23 @@ int Engine::count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts
     // a bucket list overflowed: recount with larger lists
     overflow_retries_++;
     cap_scale_ *= 2.0;
-    bucket_first_ = bucket_last_ = 0;
+    bucket_first_ = bucket_mid_ = bucket_last_ = 0;
   }
   err = "bucket lists kept overflowing";
   return PSG_ERR_INTERNAL;
+}
+
+uint64_t Engine::bucket_entries() {
+  unsigned long long v = 0;
+  cudaSetDevice(device_);
+  cudaStreamSynchronize(stream_);
+  cudaMemcpy(&v, d_entry_total_, sizeof v, cudaMemcpyDeviceToHost);
+  return v;
+}
+
+void Engine::reset_bucket_entries() {
+  cudaSetDevice(device_);
+  cudaMemset(d_entry_total_, 0, sizeof(unsigned long long));
 }
 
 std::string Engine::describe() const {

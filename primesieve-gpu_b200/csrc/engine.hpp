@@ -23,8 +23,9 @@ struct EngineConfig {
   uint32_t big_limit = 0;        // primes from: bucket sieve; 0 = auto
   uint32_t window_segments = 0;  // segments per bucket window; 0 = auto
   uint32_t bucket_lists = 0;     // lists (bucket CTAs) per segment; 0 = auto
-  uint32_t presieve = 1;         // pre-sieve with pattern tables
+  uint32_t presieve = 0;         // pre-sieve tables: 0 = default (on), 1 = on, 2 = off
   uint32_t segments_per_launch = 0; // cap on segments per sieve launch; 0 = auto
+  uint32_t sweep_limit = 0;      // big primes below: segment-major sweep; 0 = auto
 };
 
 struct KernelStat {
@@ -69,22 +70,33 @@ public:
   std::vector<KernelStat> kernel_stats();
   void reset_kernel_stats();
   uint64_t overflow_retries() const { return overflow_retries_; }
+  // Bucket entries written since the last reset (device counter; syncs).
+  uint64_t bucket_entries();
+  void reset_bucket_entries();
+  // Measured random-address shared-memory atomicAnd rate (atomics/s), the
+  // roofline denominator of the cross-off phase.
+  double measure_smem_atomic_rate();
 
 private:
   int build_presieve(std::string& err);
   int ensure_primes(uint64_t limit, std::string& err);
-  int ensure_buckets(uint32_t first_big, uint32_t last_big, std::string& err);
+  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
+  int count_enqueue(uint64_t start, uint64_t stop, uint32_t kinds,
+                    unsigned long long* dev_counts, cudaStream_t st, std::string& err);
   void timed_begin(int which, cudaStream_t st);
   void timed_end(int which, cudaStream_t st);
 
   int device_ = -1;
   cudaDeviceProp prop_{};
   cudaStream_t stream_ = nullptr;
+  cudaStream_t last_stream_ = nullptr;
+  cudaEvent_t done_event_ = nullptr;
   EngineConfig cfg_;
   uint32_t seg_bytes_ = 0, block_ = 0, grid_ = 0, bucket_block_ = 256;
   uint32_t small_limit_ = 0, big_limit_ = 0, window_ = 0, lists_ = 0;
+  uint32_t state_cap_ = 0, smem_dyn_ = 0, entry_bits_ = 20;
 
   // pre-sieve tables
   std::vector<std::vector<uint32_t>> groups_;
@@ -108,11 +120,17 @@ private:
   size_t bcounts_cap_ = 0;
   uint32_t* d_list_off_ = nullptr;
   uint32_t* d_list_cap_ = nullptr;
+  uint32_t* d_chunk_begin_ = nullptr;
   size_t lists_cap_ = 0;
   uint64_t seg_stride_ = 0;
-  uint32_t bucket_first_ = 0, bucket_last_ = 0, primes_per_list_ = 0, active_lists_ = 0;
+  uint32_t bucket_first_ = 0, bucket_mid_ = 0, bucket_last_ = 0, active_lists_ = 0;
+  uint32_t sweep_ctas_ = 0, fill_ctas_ = 0, sweep_limit_ = 0;
+  uint32_t* d_sweep_b_ = nullptr;
+  uint32_t* d_sweep_i_ = nullptr;
+  size_t sweep_state_cap_ = 0;
   double cap_scale_ = 1.0;
   uint32_t* d_overflow_ = nullptr;
+  unsigned long long* d_entry_total_ = nullptr;
   uint64_t overflow_retries_ = 0;
 
   unsigned long long* d_counts_ = nullptr;
@@ -120,8 +138,10 @@ private:
 
   // profiling
   bool profiling_ = false;
+  // launches are always counted; CUDA-event times only while profiling
   struct Timed { const char* name; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev; uint64_t launches = 0; double ms = 0; };
-  Timed timed_[2] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 } };
+  Timed timed_[3] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 },
+                      { "bucket_sweep_kernel", {}, 0, 0 } };
 };
 
 } // namespace psg

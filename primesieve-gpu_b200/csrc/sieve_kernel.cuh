@@ -1,20 +1,24 @@
 // sieve_kernel.cuh -- the segment sieve kernel (sm_100a).
 //
-// One CTA sieves one wheel-30 segment at a time in shared memory and loops
-// over segments (persistent grid). Per segment:
+// One CTA sieves one wheel-30 segment at a time in shared memory and walks a
+// contiguous stripe of segments (persistent grid), so per-prime state carries
+// from one segment to the next instead of being recomputed. Per segment:
 //   1. pre-sieve : AND of the pre-sieve patterns, 16 bytes per thread per
 //                  step, read as aligned 128-bit loads from 16 pre-shifted
 //                  copies of each pattern (L2-resident), stored with
 //                  conflict-free 128-bit shared stores.
-//   2. small     : warp-cooperative cross-off. One warp per prime; lane
+//   2. small     : warp-cooperative cross-off. One warp per prime (its
+//                  remainder segLow mod p carried in a register); lane
 //                  (j = lane&7, r = lane>>3) walks the multiples whose
 //                  cofactor is in class kCofactor[j] (mod 30), every 4th
 //                  one starting at phase r. Those multiples are p bytes
 //                  apart, so the lane strides 4p bytes = p words and its
 //                  bit (and byte-in-word) never changes: the inner loop is
 //                  one shared atomicAnd per crossing.
-//   3. medium    : one thread per prime, the same 8 progressions walked
-//                  one after the other (stride p bytes).
+//   3. medium    : one thread per prime, sequential wheel walk; each prime's
+//                  (byte position, wheel index) is kept in shared memory
+//                  between the segments of the stripe (primesieve's EratSmall/
+//                  EratMedium carry the same pair per sieving prime).
 //   4. big       : crossings streamed from the per-segment bucket lists
 //                  that the bucket kernel wrote to HBM (4-byte entries).
 //   5. count     : edge masking, __popc over the word and over shifted ANDs
@@ -31,7 +35,7 @@
 
 namespace psg {
 
-constexpr int kMaxPresieveTables = 8;
+constexpr int kMaxPresieveTables = 6;
 constexpr int kMaxPresievePrimes = 24;
 
 struct SieveArgs {
@@ -51,12 +55,14 @@ struct SieveArgs {
   const uint64_t* recip;      // floor((2^64-1)/p) per prime
   uint32_t n_small;           // primes[0, n_small): warp-cooperative
   uint32_t n_primes;          // primes[n_small, n_primes): thread per prime
+                              // (their state fits the shared-memory area)
   // big primes via buckets (num_bucket_lists == 0: none)
   const uint32_t* bucket_entries;   // [segment][seg_stride] entries
   const uint32_t* bucket_counts;    // [segment][list] number of entries
   const uint32_t* bucket_list_off;  // [list] offset inside a segment region
   uint64_t bucket_seg_stride;       // entries per segment region
   uint32_t num_bucket_lists;        // lists per segment (0: no big primes)
+  uint32_t wheel_tab[16];           // per class: bits, corr (wheel walk)
   uint32_t kinds;
   unsigned long long* counts;       // [6]
 };
@@ -137,7 +143,10 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
 {
   extern __shared__ uint4 smem4[];
   uint32_t* const sieve32 = reinterpret_cast<uint32_t*>(smem4);
+  uint32_t* const mstate = sieve32 + (a.seg_bytes >> 2);   // medium-prime state
   constexpr int NWARPS = BLOCK / 32;
+  constexpr int SREG = 2;
+  constexpr uint32_t kFar = 0xffffffffu;   // state: next multiple not representable yet
   const uint32_t tid = threadIdx.x;
   const uint32_t lane = tid & 31u;
   const uint32_t warp = tid >> 5;
@@ -145,11 +154,54 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
   const uint32_t nchunks = seg_bytes >> 4;
   const uint32_t nwords = seg_bytes >> 2;
   const uint64_t span = (uint64_t) seg_bytes * 30u;
+  const uint32_t n_med = a.n_primes - a.n_small;
+
+  // contiguous stripe of segments
+  const uint64_t per = (a.num_segments + gridDim.x - 1) / gridDim.x;
+  const uint64_t s_begin = (uint64_t) blockIdx.x * per;
+  const uint64_t s_end = (s_begin + per < a.num_segments) ? s_begin + per : a.num_segments;
 
   uint64_t acc[6] = { 0, 0, 0, 0, 0, 0 };
 
-  for (uint64_t s = blockIdx.x; s < a.num_segments; s += gridDim.x) {
+  __shared__ uint32_t wheel_tab[16];
+  __shared__ uint32_t list_next;           // bucket list dispenser (per segment)
+  if (tid < 16) wheel_tab[tid] = a.wheel_tab[tid];
+
+  // small primes of this warp, register resident: p, r = (segLow+7) mod p of
+  // the current segment, and span mod p to advance r by one segment.
+  uint32_t sp[SREG], sr[SREG], sdl[SREG];
+  {
+    const uint64_t x0 = a.seg_low0 + s_begin * span + 7;
+#pragma unroll
+    for (int m = 0; m < SREG; m++) {
+      const uint32_t idx = warp + NWARPS * (lane + 32u * m);
+      sp[m] = 1; sr[m] = 0; sdl[m] = 0;
+      if (idx < a.n_small && s_begin < s_end) {
+        const uint32_t p = a.primes[idx];
+        sp[m] = p;
+        sr[m] = mod_recip(x0, p, a.recip[idx]);
+        sdl[m] = (uint32_t) (span % p);
+      }
+    }
+  }
+
+  // medium primes: state (byte << 3 | wheel index) relative to the stripe's
+  // current segment, or kFar when the first multiple is still far away.
+  if (s_begin < s_end) {
+    const uint64_t segLow = a.seg_low0 + s_begin * span;
+    for (uint32_t i = tid; i < n_med; i += BLOCK) {
+      const uint32_t p = a.primes[a.n_small + i];
+      uint64_t d; uint32_t c0;
+      first_multiple(segLow, p, a.recip[a.n_small + i], d, c0);
+      const uint32_t j = first_class_ge(c0);
+      const uint64_t b = (d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u;
+      mstate[i] = (b < (1ull << 29) - 1) ? (uint32_t) (b << 3) | j : kFar;
+    }
+  }
+
+  for (uint64_t s = s_begin; s < s_end; s++) {
     const uint64_t segLow = a.seg_low0 + s * span;
+    if (tid == 0) list_next = 0;      // read after the next barrier
 
     // ---- 1. pre-sieve --------------------------------------------------
     {
@@ -202,16 +254,48 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
       const uint32_t j = lane & 7u;
       const uint32_t r = lane >> 3;
       const uint32_t Q = cofactor_class(j);
-      for (uint32_t i = warp; i < a.n_small; i += NWARPS) {
-        const uint32_t p = a.primes[i];
-        const uint64_t rcp = a.recip[i];
+      const uint64_t x0 = segLow + 7;
+#pragma unroll
+      for (int m = 0; m < SREG; m++) {
+        const uint32_t tbase = 32u * m;
+        if (warp + NWARPS * tbase >= a.n_small) break;
+        for (uint32_t l = 0; l < 32; l++) {
+          const uint32_t idx = warp + NWARPS * (tbase + l);
+          if (idx >= a.n_small) break;
+          const uint32_t p = __shfl_sync(0xffffffffu, sp[m], l);
+          const uint32_t rem = __shfl_sync(0xffffffffu, sr[m], l);
+          const uint32_t pm = p % 30u;
+          const uint64_t pp = (uint64_t) p * p;
+          uint64_t d; uint32_t c0;
+          if (x0 <= pp) {
+            d = pp - x0;
+            c0 = pm;
+            if (d >= span) continue;
+          } else {
+            const uint32_t dd = rem ? p - rem : 0u;
+            d = dd;
+            c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
+          }
+          const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+          const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
+          if (b64 < seg_bytes) {
+            const uint32_t b = (uint32_t) b64;
+            const uint32_t bit = residue_to_bit((Q * pm) % 30u);
+            const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
+            for (uint32_t w = b >> 2; w < nwords; w += p)
+              atomicAnd(&sieve32[w], mask);
+          }
+        }
+      }
+      // small primes beyond the register-resident ones
+      for (uint32_t idx = warp + NWARPS * 32u * SREG; idx < a.n_small; idx += NWARPS) {
+        const uint32_t p = a.primes[idx];
         uint64_t d; uint32_t c0;
-        first_multiple(segLow, p, rcp, d, c0);
+        first_multiple(segLow, p, a.recip[idx], d, c0);
         if (d >= span) continue;
         const uint32_t pm = p % 30u;
-        const uint32_t k = (Q + 30u - c0) % 30u;
-        const uint64_t off = d + (uint64_t) k * p;          // value offset
-        const uint64_t b64 = off / 30u + (uint64_t) r * p;  // byte index
+        const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+        const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
         if (b64 < seg_bytes) {
           const uint32_t b = (uint32_t) b64;
           const uint32_t bit = residue_to_bit((Q * pm) % 30u);
@@ -222,42 +306,73 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
       }
     }
 
-    // ---- 3. medium primes: one thread per prime --------------------------
-    for (uint32_t i = a.n_small + tid; i < a.n_primes; i += BLOCK) {
-      const uint32_t p = a.primes[i];
-      const uint64_t rcp = a.recip[i];
-      uint64_t d; uint32_t c0;
-      first_multiple(segLow, p, rcp, d, c0);
-      if (d / 30u >= seg_bytes) continue;
-      const uint32_t pm = p % 30u;
-#pragma unroll
-      for (uint32_t j = 0; j < 8; j++) {
-        const uint32_t Q = cofactor_class(j);
-        const uint32_t k = (Q + 30u - c0) % 30u;
-        uint64_t b = (d + (uint64_t) k * p) / 30u;
-        if (b < seg_bytes) {
-          const uint32_t bit = residue_to_bit((Q * pm) % 30u);
-          do {
-            const uint32_t bb = (uint32_t) b;
-            atomicAnd(&sieve32[bb >> 2], ~(1u << (bit + 8u * (bb & 3u))));
-            b += p;
-          } while (b < seg_bytes);
+    // ---- 3. medium primes: one thread per prime, carried wheel walk ------
+    {
+      uint32_t i = tid;
+      uint32_t p = 0;
+      if (i < n_med) p = a.primes[a.n_small + i];
+      for (; i < n_med; i += BLOCK) {
+        const uint32_t inext = i + BLOCK;
+        const uint32_t pn = (inext < n_med) ? a.primes[a.n_small + inext] : 0u;
+        uint32_t st = mstate[i];
+        if (st == kFar) {
+          uint64_t d; uint32_t c0;
+          first_multiple(segLow, p, a.recip[a.n_small + i], d, c0);
+          const uint32_t j0 = first_class_ge(c0);
+          const uint64_t b = (d + (uint64_t) (cofactor_class(j0) - c0) * p) / 30u;
+          st = (b < (1ull << 29) - 1) ? (uint32_t) (b << 3) | j0 : kFar;
         }
+        if (st != kFar) {
+          uint32_t b = st >> 3;
+          uint32_t j = st & 7u;
+          if (b < seg_bytes) {
+            const uint32_t pdiv30 = p / 30u;
+            const uint32_t cls = residue_to_bit(p - 30u * pdiv30);
+            const uint32_t bits = wheel_tab[2 * cls];
+            const uint32_t corr = wheel_tab[2 * cls + 1];
+            do {
+              const uint32_t sh = 3u * j;
+              const uint32_t bit = (bits >> sh) & 7u;
+              atomicAnd(&sieve32[b >> 2], ~(1u << (bit + 8u * (b & 3u))));
+              b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
+              j = (j + 1u) & 7u;
+            } while (b < seg_bytes);
+          }
+          const uint32_t nb = b - seg_bytes;
+          st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kFar;
+        }
+        mstate[i] = st;
+        p = pn;
       }
     }
 
     // ---- 4. big primes: bucket lists of this segment ---------------------
+    // Warps take lists from a shared counter (lists differ in length); each
+    // lane applies 4 entries per 16-byte load (lists start 16-byte aligned).
     if (a.num_bucket_lists) {
       const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
       const uint32_t* seg_entries = a.bucket_entries + s * a.bucket_seg_stride;
-      for (uint32_t l = warp; l < a.num_bucket_lists; l += NWARPS) {
+      for (;;) {
+        uint32_t l = 0;
+        if (lane == 0) l = atomicAdd(&list_next, 1u);
+        l = __shfl_sync(0xffffffffu, l, 0);
+        if (l >= a.num_bucket_lists) break;
         const uint32_t n = cnt[l];
         const uint32_t* e = seg_entries + a.bucket_list_off[l];
-        for (uint32_t x = lane; x < n; x += 32) {
-          const uint32_t v = __ldg(e + x);
-          // entry: byte index << 3 | bit
-          const uint32_t b = v >> 3;
-          atomicAnd(&sieve32[b >> 2], ~(1u << ((v & 7u) + 8u * (b & 3u))));
+        const uint32_t n4 = n & ~3u;
+        for (uint32_t x = 4 * lane; x < n4; x += 128) {
+          const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(e + x));
+          const uint32_t v[4] = { v4.x, v4.y, v4.z, v4.w };
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const uint32_t bb = v[q] >> 3;       // entry: byte index << 3 | bit
+            atomicAnd(&sieve32[bb >> 2], ~(1u << ((v[q] & 7u) + 8u * (bb & 3u))));
+          }
+        }
+        if (n4 + lane < n) {
+          const uint32_t v = __ldg(e + n4 + lane);
+          const uint32_t bb = v >> 3;
+          atomicAnd(&sieve32[bb >> 2], ~(1u << ((v & 7u) + 8u * (bb & 3u))));
         }
       }
     }
@@ -292,6 +407,13 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
       }
 #pragma unroll
       for (int k = 0; k < 6; k++) acc[k] += c[k];
+    }
+
+    // advance the small primes' remainders to the next segment
+#pragma unroll
+    for (int m = 0; m < SREG; m++) {
+      const uint32_t nr = sr[m] + sdl[m];
+      sr[m] = (nr >= sp[m]) ? nr - sp[m] : nr;
     }
     __syncthreads();
   }

@@ -69,18 +69,60 @@ PSG_HD uint32_t inverse_mod30(uint32_t r) {
   return (uint32_t) ((w >> (5 * (r % 12))) & 31u);
 }
 
-// Bit mask of a byte that keeps the values >= segLow + 30*i + x (x is the
-// offset of the first wanted value inside the byte, clamped to 0..32).
-PSG_HD uint32_t keep_from(uint32_t x) {
-  uint32_t m = 0;
-  for (int j = 0; j < 8; j++) if (kBitValue[j] >= x) m |= 1u << j;
-  return m;
+// ---- wheel walk tables ----------------------------------------------------
+// Walking the multiples p*q of a sieving prime p in increasing order, the
+// cofactor q steps through the classes kCofactor[j] with gaps
+// {6,4,2,4,2,4,6,2}. With p = 30*pdiv30 + pm, the byte index of the next
+// multiple grows by pdiv30*gap_j + corr_j(pm), and its bit is bit_j(pm).
+// Both depend only on the class of pm (8 classes, indexed by
+// residue_to_bit(pm)); they are packed 3 bits per j.
+constexpr uint32_t kGapPacked = 6u | (4u << 3) | (2u << 6) | (4u << 9) | (2u << 12) |
+                                (4u << 15) | (6u << 18) | (2u << 21);
+
+constexpr uint32_t value_offset_of_residue(uint32_t r) { return r < 7 ? r + 30 : r; }
+
+constexpr uint32_t class_residue(uint32_t c) { return c == 7 ? 1u : kBitValue[c]; }
+
+constexpr uint32_t bit_of_residue_c(uint32_t r) {
+  uint32_t b = 0;
+  for (uint32_t j = 0; j < 8; j++) if (kBitValue[j] % 30 == r) b = j;
+  return b;
 }
-// ... and the values <= segLow + 30*i + x.
-PSG_HD uint32_t keep_upto(uint32_t x) {
-  uint32_t m = 0;
-  for (int j = 0; j < 8; j++) if (kBitValue[j] <= x) m |= 1u << j;
-  return m;
+
+constexpr uint32_t wheel_bits_packed(uint32_t c) {
+  uint32_t v = 0;
+  for (uint32_t j = 0; j < 8; j++)
+    v |= bit_of_residue_c((class_residue(c) * kCofactor[j]) % 30) << (3 * j);
+  return v;
+}
+
+constexpr uint32_t wheel_corr_packed(uint32_t c) {
+  uint32_t v = 0;
+  const uint32_t pm = class_residue(c);
+  for (uint32_t j = 0; j < 8; j++) {
+    const uint32_t gap = (kGapPacked >> (3 * j)) & 7u;
+    const uint32_t vj = value_offset_of_residue((pm * kCofactor[j]) % 30);
+    const uint32_t vn = value_offset_of_residue((pm * kCofactor[(j + 1) & 7]) % 30);
+    v |= ((vj + pm * gap - vn) / 30) << (3 * j);
+  }
+  return v;
+}
+
+// c0 (cofactor residue 0..29) -> first class j with kCofactor[j] >= c0.
+constexpr uint64_t first_class_packed(int part) {
+  uint64_t v = 0;
+  for (int c = 0; c < 30; c++) {
+    int j = 0;
+    while (kCofactor[j] < (uint32_t) c) j++;
+    if (c / 20 == part) v |= (uint64_t) j << (3 * (c % 20));
+  }
+  return v;
+}
+constexpr uint64_t kFirstClass0 = first_class_packed(0);
+constexpr uint64_t kFirstClass1 = first_class_packed(1);
+
+PSG_HD uint32_t first_class_ge(uint32_t c0) {
+  return (uint32_t) ((c0 < 20 ? (kFirstClass0 >> (3 * c0)) : (kFirstClass1 >> (3 * (c0 - 20)))) & 7u);
 }
 
 // ---- count kinds --------------------------------------------------------

@@ -1,0 +1,179 @@
+"""GPU parity: every count from the CUDA path (through the C ABI, the
+primesieve C API, the C++ API and the CLI) equals the reference's counts
+bit for bit: the reference's own golden vectors, counts computed by the
+reference's CPU library, and the oracle on the same seeded inputs."""
+import ctypes
+import os
+import random
+import subprocess
+
+import pytest
+
+from conftest import REPO, PKG_DIR
+
+pytestmark = pytest.mark.gpu
+
+
+def test_reference_computed_cases(ctx, ref_counts):
+    """test/gpu_count.cpp case list (every kind at 18 small stops, every start
+    residue mod 30, segment boundaries near 1e9, five larger ranges), edges
+    near 2^32, 2^63 and 2^64, and seeded random ranges."""
+    by_range = {}
+    for c in ref_counts["cases"]:
+        by_range.setdefault((c["start"], c["stop"]), []).append(c)
+    for (a, b), cs in by_range.items():
+        got = ctx.count(a, b)
+        for c in cs:
+            assert got[c["kind"]] == c["count"], (a, b, c, got)
+
+
+def test_reference_vectors(ctx, ref_vectors):
+    """Known answers from the reference's tests, including the stress-test
+    tables (99 windows of 1e11 at 1e13 and at 1e19)."""
+    by_range = {}
+    for v in ref_vectors:
+        by_range.setdefault((v["start"], v["stop"]), []).append(v)
+    for (a, b), vs in sorted(by_range.items()):
+        kinds = 0
+        for v in vs:
+            kinds |= 1 << v["kind"]
+        got = ctx.count(a, b, kinds)
+        for v in vs:
+            assert got[v["kind"]] == v["count"], (v, got)
+
+
+def test_benchmark_workloads(ctx, ref_counts):
+    """pi(1e9); [1e15, 1e15+1e11]; [0, 1e11]; [2^64-2^34, 2^64-1] ... all six
+    counts each, against the reference CPU library."""
+    for row in ref_counts["bench"]:
+        assert ctx.count(row["start"], row["stop"]) == row["counts"], row
+
+
+def test_oracle_random_ranges(ctx, oracle):
+    rng = random.Random(7)
+    for base in [0, 10 ** 5, 10 ** 8, 10 ** 10, 10 ** 12, 2 ** 40]:
+        for _ in range(10):
+            a = base + rng.randrange(10 ** 6)
+            b = a + rng.randrange(2 * 10 ** 6)
+            assert ctx.count(a, b) == oracle.plain(a, b), (a, b)
+
+
+CONFIGS = [
+    dict(seg_bytes=4096, block=256),                        # many tiny segments
+    dict(seg_bytes=8192, block=512, presieve=2),            # no pre-sieve
+    dict(seg_bytes=16384, block=256, small_limit=64),       # no warp-cooperative tier
+    dict(seg_bytes=16384, block=256, small_limit=100000),   # only warp-cooperative
+    dict(seg_bytes=4096, block=256, big_limit=200, window_segments=3, bucket_lists=5),
+    dict(seg_bytes=65536, block=1024, big_limit=1000, window_segments=7),
+    dict(seg_bytes=4096, block=256, big_limit=300, sweep_limit=3000, window_segments=5),   # sweep + fill
+    dict(seg_bytes=16384, block=512, big_limit=500, sweep_limit=500, bucket_lists=3),      # fill only
+    dict(seg_bytes=32768, block=512, ctas_per_sm=2),
+]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=[str(c) for c in CONFIGS])
+def test_engine_configs(psg, oracle, ref_counts, cfg):
+    """Segment sizes, block sizes, tier limits, bucket windows and list
+    counts change the work split, never the result."""
+    c = psg.Context(**cfg)
+    try:
+        rng = random.Random(11)
+        ranges = [(0, 10 ** 6), (0, 1000), (999999900, 1000000231), (10 ** 12, 10 ** 12 + 10 ** 6)]
+        ranges += [(x, x + rng.randrange(3 * 10 ** 5)) for x in
+                   (rng.randrange(10 ** 13) for _ in range(6))]
+        for a, b in ranges:
+            assert c.count(a, b) == oracle.plain(a, b), (cfg, a, b)
+        top = 2 ** 64 - 1
+        row = [r for r in ref_counts["cases"] if r["start"] == top - 10 ** 6 and r["stop"] == top]
+        got = c.count(top - 10 ** 6, top)
+        for r in row:
+            assert got[r["kind"]] == r["count"]
+    finally:
+        c.close()
+
+
+def test_additivity_full_size(ctx, ref_counts, psg):
+    """Size-independent property at the benchmark size: the six counts of
+    [1e15, 1e15+1e11] equal the sum over 5 shards cut at == 2 (mod 30)."""
+    row = [r for r in ref_counts["bench"] if r["start"] == 10 ** 15 and r["stop"] == 10 ** 15 + 10 ** 11][0]
+    total = [0] * 6
+    for a, b in psg.split_range(row["start"], row["stop"], 5):
+        total = [t + c for t, c in zip(total, ctx.count(a, b))]
+    assert total == row["counts"]
+
+
+def test_empty_and_single(ctx):
+    assert ctx.count(10, 5) == [0] * 6
+    assert ctx.count(0, 0) == [0] * 6
+    assert ctx.count(2, 2) == [1, 0, 0, 0, 0, 0]
+    assert ctx.count(7, 7) == [1, 0, 0, 0, 0, 0]
+    assert ctx.count(2 ** 64 - 1, 2 ** 64 - 1) == [0] * 6
+    assert ctx.count(2 ** 64 - 59, 2 ** 64 - 59)[0] == 1      # largest 64-bit prime
+    assert ctx.count(0, 100, 0) == [0] * 6                    # no kinds requested
+    assert ctx.count(0, 100, 1 << 2) == [0, 0, 8, 0, 0, 0]    # one kind only
+
+
+def test_batch_matches_single(ctx):
+    ranges = [(0, 10 ** 7, 63), (10 ** 12, 10 ** 12 + 10 ** 7, 1), (5, 4, 63), (2 ** 64 - 10 ** 5, 2 ** 64 - 1, 6)]
+    got = ctx.count_batch(ranges)
+    for (a, b, k), g in zip(ranges, got):
+        assert g == ctx.count(a, b, k)
+
+
+def test_count_async_accumulates(ctx, psg):
+    import torch
+    dev = torch.zeros(6, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+    ctx.count_async(0, 10 ** 8, 63, dev.data_ptr(), stream.cuda_stream)
+    ctx.count_async(0, 10 ** 8, 63, dev.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    assert [x // 2 for x in dev.tolist()] == ctx.count(0, 10 ** 8)
+
+
+def test_c_api(psg, ctx):
+    lib = psg.load()
+    a, b = 10 ** 12, 10 ** 12 + 10 ** 8
+    want = ctx.count(a, b)
+    for k, name in enumerate(psg.KIND_NAMES):
+        assert getattr(lib, "primesieve_count_" + name)(a, b) == want[k]
+    out = (ctypes.c_uint64 * 6)()
+    assert lib.primesieve_count_all(ctypes.c_uint64(a), ctypes.c_uint64(b), out) == 0
+    assert list(out) == want
+    lib.primesieve_get_max_stop.restype = ctypes.c_uint64
+    assert lib.primesieve_get_max_stop() == 2 ** 64 - 1
+
+
+def test_cpp_api(tmp_path, ctx):
+    exe = tmp_path / "api_check"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "cpp", "api_check.cpp"), "-o", str(exe),
+                    "-L", os.path.join(PKG_DIR, "lib"), "-lprimesieve_gpu",
+                    "-Wl,-rpath," + os.path.join(PKG_DIR, "lib")], check=True)
+    a, b = 10 ** 9, 10 ** 9 + 10 ** 7
+    out = subprocess.run([str(exe), str(a), str(b)], capture_output=True, text=True, check=True).stdout
+    lines = dict(l.split(" ", 1) for l in out.strip().split("\n"))
+    want = " ".join(str(x) for x in ctx.count(a, b))
+    assert lines["count"] == want and lines["gpu"] == want and lines["all"] == want
+    assert lines["knobs"] == f"1 {ctx.count(a, b)[0]}"
+    assert lines["worthwhile"] == "1 0"
+
+
+def cli(*args):
+    return subprocess.run([os.path.join(PKG_DIR, "bin", "primesieve"), *args], capture_output=True, text=True)
+
+
+def test_cli(ref_counts):
+    r = cli("1e12", "1e12+1e9", "-c123456", "--gpu")
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().split("\n")
+    assert lines[0].startswith("GPU = ") and lines[1].startswith("Seconds: ")
+    assert lines[2:] == ["Primes: 36190991", "Twin primes: 1730012", "Prime triplets: 271316",
+                         "Prime quadruplets: 7171", "Prime quintuplets: 1259", "Prime sextuplets: 42"]
+    r = cli("1e9", "--count", "--gpu", "-q")
+    assert r.returncode == 0 and r.stdout == "50847534\n"
+    r = cli("1e10", "--dist=1e3", "-c12", "-q")
+    assert r.stdout == "Primes: 44\nTwin primes: 2\n"
+    r = cli("100", "10", "-q")
+    assert r.stdout == "0\n"
+    r = cli("18446744056529682432", "18446744073709551615", "-c6", "-q", "--time")
+    assert r.returncode == 0 and r.stdout.split("\n")[1] == "39"
