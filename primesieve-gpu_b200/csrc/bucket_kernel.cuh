@@ -122,6 +122,13 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   uint32_t b = kDone, p = 0, ebit = 0;    // this lane's progression
   uint32_t group = warp;                  // next group of 4 primes of this warp
   bool warp_done = false;
+  // prefetched prime of the next group (its loads overlap the current walk)
+  uint32_t p_nx = 0;
+  uint64_t r_nx = 0;
+  {
+    const uint32_t idx = lo + group * 4u + g;
+    if (idx < hi) { p_nx = a.primes[idx]; r_nx = a.recip[idx]; }
+  }
 
   for (;;) {
     // ---- 1. generate: kFillSteps steps per warp into the tile
@@ -132,10 +139,16 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
         if (base >= hi) { warp_done = true; break; }
         group += NWARPS;
         const uint32_t idx = base + g;
+        const uint32_t p_cur = p_nx;
+        const uint64_t r_cur = r_nx;
+        {
+          const uint32_t nidx = lo + group * 4u + g;
+          if (nidx < hi) { p_nx = a.primes[nidx]; r_nx = a.recip[nidx]; }
+        }
         if (idx < hi) {
-          p = a.primes[idx];
+          p = p_cur;
           uint64_t d; uint32_t c0;
-          first_multiple(a.win_low, p, a.recip[idx], d, c0);
+          first_multiple(a.win_low, p, r_cur, d, c0);
           const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
           const uint64_t b64 = (d + (uint64_t) k * p) / 30u;   // byte index in window
           if (b64 < win_bytes) b = (uint32_t) b64;

@@ -273,7 +273,7 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   small_limit_ = cfg.small_limit ? cfg.small_limit : 4096u;
   big_limit_ = cfg.big_limit ? cfg.big_limit : (uint32_t) std::min<uint64_t>(span / 10u, 0xffffffffull);
   if (big_limit_ < small_limit_) big_limit_ = small_limit_;
-  window_ = cfg.window_segments ? cfg.window_segments : grid_ * 4u;
+  window_ = cfg.window_segments ? cfg.window_segments : grid_ * 8u;
   // the bucket fill kernel scans W <= 8 * its block size segment counters
   // and packs (segment, byte << 3 | bit) into 32 bits
   entry_bits_ = 3;
