@@ -132,6 +132,24 @@ int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset);
  * random-address shared-memory atomicAnd on this device (atomics/s). */
 int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s);
 
+/* Count without allocating anything (no reference counterpart: the
+ * reference always allocates through its backend). For callers that cannot
+ * allocate device memory when they count -- inside CUDA graph capture,
+ * allocator callbacks, real-time loops, fixed-budget embedders. Same result
+ * as psg_count(), written (overwritten) to dev_counts, a device buffer of 6
+ * uint64_t, on `stream` (a cudaStream_t; NULL = the legacy default stream).
+ * Runs on the current device; no context is needed.
+ *   Limit: stop <= 2^36 (PSG_ERR_LIMIT beyond). No cudaMalloc or cudaFree:
+ *   the sieving primes <= 2^18, their reciprocals and the count accumulators
+ *   live in one fixed static device array of about 270 KiB that every GPU
+ *   loading the library keeps until the process exits.
+ *   The first call on a device sets that array up synchronously (symbol
+ *   lookup, table copy, one kernel); make it before any stream capture.
+ *   All calls share the array, so calls that overlap on the GPU (different
+ *   streams, different host threads) race; serialise them. */
+int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
+                      uint64_t* dev_counts, void* stream);
+
 /* The library version string. */
 const char* psg_version(void);
 

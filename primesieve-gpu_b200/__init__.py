@@ -27,7 +27,7 @@ PSG_SYMBOLS = (
     "psg_get_config", "psg_describe", "psg_count", "psg_count_async",
     "psg_count_batch", "psg_prepare", "psg_last_error", "psg_status_string",
     "psg_set_profiling", "psg_kernel_stats", "psg_reset_kernel_stats", "psg_version",
-    "psg_bucket_entries", "psg_measure_smem_atomic_rate",
+    "psg_bucket_entries", "psg_measure_smem_atomic_rate", "psg_count_noalloc",
 )
 
 
@@ -84,6 +84,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_reset_kernel_stats.argtypes = [vp]
     lib.psg_bucket_entries.argtypes = [vp, U64P, i32]
     lib.psg_measure_smem_atomic_rate.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    lib.psg_count_noalloc.argtypes = [u64, u64, u32, vp, vp]
     lib.psg_version.restype = ctypes.c_char_p
     for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
         fn = getattr(lib, "primesieve_count_" + name, None)

@@ -46,6 +46,11 @@ psg::EngineConfig to_engine(const psg_config* c) {
 
 } // namespace
 
+namespace psg {
+// Lets other translation units of the library report through psg_last_error().
+void set_last_error(const std::string& msg) { t_last_error = msg; }
+}
+
 extern "C" {
 
 const char* psg_version(void) { return "primesieve-b200 1.0 (primesieve 12.16 count API)"; }
