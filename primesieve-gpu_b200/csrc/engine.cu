@@ -3,6 +3,7 @@
 #include "sieve_kernel.cuh"
 #include "bucket_kernel.cuh"
 #include "sweep_kernel.cuh"
+#include "primegen_kernel.cuh"
 #include "../../include/psgpu.h"
 
 #include <algorithm>
@@ -76,6 +77,11 @@ __global__ void recip_kernel(const uint32_t* __restrict__ p, uint64_t* __restric
   for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n;
        i += (size_t) gridDim.x * blockDim.x)
     r[i] = 0xffffffffffffffffull / p[i];
+}
+
+__global__ void gather_kernel(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, size_t n, size_t stride) {
+  for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = src[i * stride];
 }
 
 __global__ void add_counts_kernel(unsigned long long* c, unsigned long long a0, unsigned long long a1,
@@ -284,6 +290,7 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   window_ = std::min<uint32_t>(window_, (uint32_t) ((1ull << 31) / seg_bytes_));
   cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int) fill_smem_bytes<kBucketBlock>(window_));
+  cudaFuncSetAttribute(primegen_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, 131072);
   cudaFuncSetAttribute(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (window_ * sizeof(uint32_t)));
   // sweep primes need pdiv30 < 2^22 (state packing): p < 1.25e8
@@ -348,42 +355,158 @@ int Engine::build_presieve(std::string& err) {
   return PSG_OK;
 }
 
+// Grow the device table d_primes_/d_recip_ to hold n primes (keeping the
+// first keep entries).
+int Engine::reserve_primes(size_t n, size_t keep, std::string& err) {
+  if (n <= d_primes_cap_) return PSG_OK;
+  uint32_t* np = nullptr; uint64_t* nr = nullptr;
+  const size_t cap = std::max<size_t>(n, 1024);
+  PSG_CUDA(cudaMalloc(&np, cap * sizeof(uint32_t)));
+  PSG_CUDA(cudaMalloc(&nr, cap * sizeof(uint64_t)));
+  if (keep) {
+    PSG_CUDA(cudaMemcpyAsync(np, d_primes_, keep * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
+    PSG_CUDA(cudaMemcpyAsync(nr, d_recip_, keep * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream_));
+  }
+  PSG_CUDA(cudaStreamSynchronize(stream_));
+  cudaFree(d_primes_); cudaFree(d_recip_);
+  d_primes_ = np; d_recip_ = nr; d_primes_cap_ = cap;
+  return PSG_OK;
+}
+
+// Sieving primes (presieve_max_, limit]. Up to kHostExact they are made on
+// the host (exact host copy h_primes_, used for tier limits and bucket
+// planning); beyond, on the device by primegen_kernel (two passes: count per
+// segment, then write at the scanned offsets), with a 1-in-kSample host
+// sample of the whole table for lookups and planning.
 int Engine::ensure_primes(uint64_t limit, std::string& err) {
   if (limit <= primes_upto_ && d_primes_) return PSG_OK;
   // grow geometrically so repeated calls with rising stops stay cheap
   uint64_t target = std::max<uint64_t>(limit, std::min<uint64_t>(primes_upto_ * 2, 0xffffffffull));
   target = std::max<uint64_t>(target, 1u << 16);
   target = std::min<uint64_t>(target, 0xffffffffull);
-  const uint32_t after = std::max<uint32_t>(presieve_max_, (uint32_t) std::min<uint64_t>(primes_upto_, 0xffffffffull));
-  std::vector<uint32_t> more;
-  host_primes(after, (uint32_t) target, more);
-  const size_t old_n = h_primes_.size();
-  h_primes_.insert(h_primes_.end(), more.begin(), more.end());
-  primes_upto_ = target;
-  const size_t n = h_primes_.size();
-  if (n > d_primes_cap_) {
-    uint32_t* np = nullptr; uint64_t* nr = nullptr;
-    size_t cap = std::max<size_t>(n, 1024);
-    PSG_CUDA(cudaMalloc(&np, cap * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&nr, cap * sizeof(uint64_t)));
-    if (old_n) {
-      PSG_CUDA(cudaMemcpyAsync(np, d_primes_, old_n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream_));
-      PSG_CUDA(cudaMemcpyAsync(nr, d_recip_, old_n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream_));
+
+  // ---- host part (exact): up to kHostExact
+  if (primes_upto_ < kHostExact || !d_primes_) {
+    const uint64_t htarget = std::min<uint64_t>(target, kHostExact);
+    const uint32_t after = std::max<uint32_t>(presieve_max_, (uint32_t) primes_upto_);
+    std::vector<uint32_t> more;
+    host_primes(after, (uint32_t) htarget, more);
+    const size_t old_n = n_dev_;
+    const size_t n = old_n + more.size();
+    int rc = reserve_primes(n, old_n, err);
+    if (rc) return rc;
+    h_primes_.insert(h_primes_.end(), more.begin(), more.end());
+    if (n > old_n) {
+      PSG_CUDA(cudaMemcpyAsync(d_primes_ + old_n, h_primes_.data() + old_n, (n - old_n) * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, stream_));
+      const size_t m = n - old_n;
+      recip_kernel<<<(uint32_t) std::min<size_t>((m + 255) / 256, 4096), 256, 0, stream_>>>(d_primes_ + old_n, d_recip_ + old_n, m);
+      PSG_CUDA(cudaGetLastError());
+      PSG_CUDA(cudaStreamSynchronize(stream_));
     }
-    PSG_CUDA(cudaStreamSynchronize(stream_));
-    cudaFree(d_primes_); cudaFree(d_recip_);
-    d_primes_ = np; d_recip_ = nr; d_primes_cap_ = cap;
+    n_dev_ = n;
+    primes_upto_ = htarget;
   }
-  if (n > old_n) {
-    PSG_CUDA(cudaMemcpyAsync(d_primes_ + old_n, h_primes_.data() + old_n, (n - old_n) * sizeof(uint32_t),
-                             cudaMemcpyHostToDevice, stream_));
-    const size_t m = n - old_n;
-    const uint32_t g = (uint32_t) std::min<size_t>((m + 255) / 256, 4096);
-    recip_kernel<<<g, 256, 0, stream_>>>(d_primes_ + old_n, d_recip_ + old_n, m);
-    PSG_CUDA(cudaGetLastError());
-    PSG_CUDA(cudaStreamSynchronize(stream_));
+
+  // ---- device part: (primes_upto_, target]
+  if (target > primes_upto_) {
+    const uint64_t lo = primes_upto_ + 1, hi = target;
+    // base primes 7 .. sqrt(hi) (<= 2^16): the pre-sieve primes + the head
+    std::vector<uint32_t> base;
+    const uint32_t r = isqrt64(hi);
+    host_primes(6, std::min<uint32_t>(presieve_max_, r), base);
+    for (uint32_t q : h_primes_) { if (q > r) break; base.push_back(q); }
+    uint32_t n_small = 0;
+    while (n_small < base.size() && base[n_small] < 1024u) n_small++;
+    const uint32_t seg = 131072u;                       // primegen segment, 1024 threads
+    const uint64_t span = (uint64_t) seg * 30u;
+    const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
+    const uint32_t nseg = (uint32_t) ((hi - 7 - seg_low0) / span + 1);
+    uint32_t* d_base = nullptr; uint64_t* d_brecip = nullptr;
+    uint32_t* d_cnt = nullptr; uint64_t* d_off = nullptr;
+    auto cleanup = [&]() { cudaFree(d_base); cudaFree(d_brecip); cudaFree(d_cnt); cudaFree(d_off); };
+    if (cudaMalloc(&d_base, base.size() * 4) != cudaSuccess || cudaMalloc(&d_brecip, base.size() * 8) != cudaSuccess ||
+        cudaMalloc(&d_cnt, (size_t) nseg * 4) != cudaSuccess || cudaMalloc(&d_off, (size_t) nseg * 8) != cudaSuccess) {
+      cudaGetLastError(); cleanup();
+      err = "cannot allocate the prime generator's buffers";
+      return PSG_ERR_NOMEM;
+    }
+    PrimeGenArgs g;
+    std::memset(&g, 0, sizeof g);
+    g.seg_low0 = seg_low0; g.lo = lo; g.hi = hi; g.num_segments = nseg; g.seg_bytes = seg;
+    g.base = d_base; g.base_recip = d_brecip; g.n_base_small = n_small; g.n_base = (uint32_t) base.size();
+    g.seg_counts = d_cnt; g.seg_offsets = d_off;
+    for (uint32_t c = 0; c < 8; c++) { g.wheel_tab[2 * c] = wheel_bits_packed(c); g.wheel_tab[2 * c + 1] = wheel_corr_packed(c); }
+    cudaError_t e = cudaMemcpyAsync(d_base, base.data(), base.size() * 4, cudaMemcpyHostToDevice, stream_);
+    recip_kernel<<<64, 256, 0, stream_>>>(d_base, d_brecip, base.size());
+    const uint32_t grid = std::min<uint32_t>(nseg, (uint32_t) prop_.multiProcessorCount);
+    g.pass = 0;
+    primegen_kernel<1024><<<grid, 1024, seg, stream_>>>(g);
+    std::vector<uint32_t> cnt(nseg);
+    std::vector<uint64_t> off(nseg);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), d_cnt, (size_t) nseg * 4, cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) { cleanup(); err = std::string("prime generator (count): ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < nseg; i++) { off[i] = total; total += cnt[i]; }
+    const size_t old_n = n_dev_;
+    int rc = reserve_primes(old_n + total, old_n, err);
+    if (rc) { cleanup(); return rc; }
+    e = cudaMemcpyAsync(d_off, off.data(), (size_t) nseg * 8, cudaMemcpyHostToDevice, stream_);
+    g.pass = 1;
+    g.out = d_primes_ + old_n;
+    primegen_kernel<1024><<<grid, 1024, seg, stream_>>>(g);
+    if (total)
+      recip_kernel<<<(uint32_t) std::min<uint64_t>((total + 255) / 256, 4096), 256, 0, stream_>>>(d_primes_ + old_n, d_recip_ + old_n, total);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cleanup();
+    if (e != cudaSuccess) { err = std::string("prime generator (write): ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+    n_dev_ = old_n + total;
+    primes_upto_ = target;
+  }
+
+  // ---- 1-in-kSample host sample of the whole table (gathered on the device)
+  const size_t ns = (n_dev_ + kSample - 1) / kSample;
+  h_sample_.resize(ns);
+  if (ns) {
+    uint32_t* d_s = nullptr;
+    PSG_CUDA(cudaMalloc(&d_s, ns * sizeof(uint32_t)));
+    gather_kernel<<<(uint32_t) std::min<size_t>((ns + 255) / 256, 4096), 256, 0, stream_>>>(d_primes_, d_s, ns, kSample);
+    cudaError_t e = cudaMemcpyAsync(h_sample_.data(), d_s, ns * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    cudaFree(d_s);
+    if (e != cudaSuccess) { err = std::string("prime sample: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
   }
   return PSG_OK;
+}
+
+// Number of table primes <= v (strict = false) or < v (strict = true).
+uint32_t Engine::count_primes_le(uint64_t v, bool strict) {
+  const uint32_t x = (uint32_t) std::min<uint64_t>(v, 0xffffffffull);
+  if (v <= kHostExact || v <= (h_primes_.empty() ? 0 : h_primes_.back())) {
+    auto it = strict ? std::lower_bound(h_primes_.begin(), h_primes_.end(), x)
+                     : std::upper_bound(h_primes_.begin(), h_primes_.end(), x);
+    if (it != h_primes_.end() || n_dev_ == h_primes_.size()) return (uint32_t) (it - h_primes_.begin());
+  }
+  // beyond the exact head: locate the sample block, then fetch that block
+  auto it = strict ? std::lower_bound(h_sample_.begin(), h_sample_.end(), x)
+                   : std::upper_bound(h_sample_.begin(), h_sample_.end(), x);
+  const size_t k = (size_t) (it - h_sample_.begin());
+  if (k == 0) return 0;
+  const size_t b0 = (k - 1) * kSample;
+  const size_t b1 = std::min<size_t>(b0 + kSample, n_dev_);
+  uint32_t blk[kSample];
+  cudaMemcpy(blk, d_primes_ + b0, (b1 - b0) * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  auto jt = strict ? std::lower_bound(blk, blk + (b1 - b0), x) : std::upper_bound(blk, blk + (b1 - b0), x);
+  return (uint32_t) (b0 + (size_t) (jt - blk));
+}
+
+// Table prime i for planning: exact in the host head, else the smallest prime
+// of its sample block (a slight underestimate).
+double Engine::approx_prime(uint32_t i) const {
+  if (i < h_primes_.size()) return (double) h_primes_[i];
+  return (double) h_sample_[std::min<size_t>(i / kSample, h_sample_.size() - 1)];
 }
 
 int Engine::prepare(uint64_t stop, std::string& err) {
@@ -423,7 +546,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     std::vector<double> mu(sweep_ctas, 0.0);
     for (uint32_t idx = 0; idx < nsweep; idx++) {
       const uint32_t gw = (idx / 32u) % nw_launch;
-      mu[gw / kSweepWarps] += per_seg / (double) h_primes_[first + idx];
+      mu[gw / kSweepWarps] += per_seg / approx_prime(first + idx);
     }
     const double mu_max = *std::max_element(mu.begin(), mu.end());
     for (uint32_t c = 0; c < sweep_ctas; c++) add_list(mu_max);
@@ -434,23 +557,41 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
   uint32_t fill_ctas = 0;
   if (nfill) {
     fill_ctas = std::max<uint32_t>(1, std::min<uint32_t>(lists_, nfill));
-    const double win_span = span * (double) window_;
+    const double win_span = span * (8.0 / 30.0) * (double) window_;
     const double setup = 8.0;
+    // pieces [i0, i1) with their sum of 1/p: single primes inside the exact
+    // host head, whole sample blocks beyond it
+    std::vector<uint32_t> pc_begin;
+    std::vector<double> pc_inv;
+    for (uint32_t i = mid; i < last;) {
+      uint32_t j;
+      double inv;
+      if (i < h_primes_.size()) { j = i + 1; inv = 1.0 / (double) h_primes_[i]; }
+      else {
+        j = std::min<uint32_t>(last, (uint32_t) ((i / kSample + 1) * kSample));
+        inv = (double) (j - i) / approx_prime(i);
+      }
+      pc_begin.push_back(i);
+      pc_inv.push_back(inv);
+      i = j;
+    }
+    pc_begin.push_back(last);
     double total = 0;
-    for (uint32_t i = mid; i < last; i++) total += setup + win_span * (8.0 / 30.0) / (double) h_primes_[i];
+    for (size_t q = 0; q + 1 < pc_begin.size(); q++)
+      total += setup * (pc_begin[q + 1] - pc_begin[q]) + win_span * pc_inv[q];
     begin.assign(fill_ctas + 1, last);
     begin[0] = mid;
+    std::vector<double> mu(fill_ctas, 0.0);
     double acc = 0;
     uint32_t l = 1;
-    for (uint32_t i = mid; i < last && l < fill_ctas; i++) {
-      acc += setup + win_span * (8.0 / 30.0) / (double) h_primes_[i];
-      if (acc >= total * (double) l / (double) fill_ctas) begin[l++] = i + 1;
+    for (size_t q = 0; q + 1 < pc_begin.size(); q++) {
+      mu[l - 1] += per_seg * pc_inv[q];
+      acc += setup * (pc_begin[q + 1] - pc_begin[q]) + win_span * pc_inv[q];
+      if (l < fill_ctas && acc >= total * (double) l / (double) fill_ctas) begin[l++] = pc_begin[q + 1];
     }
-    for (uint32_t c = 0; c < fill_ctas; c++) {
-      double mu = 0;
-      for (uint32_t i = begin[c]; i < begin[c + 1]; i++) mu += per_seg / (double) h_primes_[i];
-      add_list(mu);
-    }
+    for (; l < fill_ctas; l++) begin[l] = last;
+    begin[fill_ctas] = last;
+    for (uint32_t c = 0; c < fill_ctas; c++) add_list(mu[c]);
   }
   const uint32_t lists = sweep_ctas + fill_ctas;
   if (stride > 0xffffffffull) { err = "bucket region too large"; return PSG_ERR_LIMIT; }
@@ -548,12 +689,8 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
   int rc = ensure_primes(std::max<uint32_t>(sq, 7u), err);
   if (rc) return rc;
 
-  const auto upto = [&](uint64_t v) {
-    return (uint32_t) (std::upper_bound(h_primes_.begin(), h_primes_.end(), (uint32_t) std::min<uint64_t>(v, 0xffffffffull)) - h_primes_.begin());
-  };
-  const auto below = [&](uint64_t v) {
-    return (uint32_t) (std::lower_bound(h_primes_.begin(), h_primes_.end(), (uint32_t) std::min<uint64_t>(v, 0xffffffffull)) - h_primes_.begin());
-  };
+  const auto upto = [&](uint64_t v) { return count_primes_le(v, false); };
+  const auto below = [&](uint64_t v) { return count_primes_le(v, true); };
   const uint32_t n_total = upto(sq);
   const uint32_t n_small = std::min(below(small_limit_), n_total);
   // medium primes must fit the shared-memory state area; the rest go to buckets

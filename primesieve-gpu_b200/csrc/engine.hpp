@@ -80,6 +80,9 @@ public:
 private:
   int build_presieve(std::string& err);
   int ensure_primes(uint64_t limit, std::string& err);
+  int reserve_primes(size_t n, size_t keep, std::string& err);
+  uint32_t count_primes_le(uint64_t v, bool strict);
+  double approx_prime(uint32_t i) const;
   int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
@@ -106,8 +109,13 @@ private:
   std::vector<uint32_t> presieve_primes_;
   uint32_t presieve_max_ = 0;
 
-  // sieving primes > presieve_max_, ascending
+  // sieving primes > presieve_max_, ascending: all on the device (n_dev_);
+  // exact host copy up to kHostExact, 1-in-kSample host sample of all
+  static constexpr uint64_t kHostExact = 1ull << 24;
+  static constexpr size_t kSample = 256;
   std::vector<uint32_t> h_primes_;
+  std::vector<uint32_t> h_sample_;
+  size_t n_dev_ = 0;
   uint64_t primes_upto_ = 0;
   uint32_t* d_primes_ = nullptr;
   uint64_t* d_recip_ = nullptr;
