@@ -1,0 +1,223 @@
+// batch.cu -- Engine::count_batch: many ranges in one persistent launch.
+//
+// Plan (host, once per batch):
+//  * 2/3/5 table per range on the host, as in count();
+//  * one sieving-prime table for the largest stop;
+//  * per range its prime tiers (small / medium with carried state / direct)
+//    and its class: a range whose primes beyond the shared state are few
+//    enough for its length (segments x such primes <= kDirectBudget) is
+//    sieved entirely by the persistent batch kernel; longer ranges with many
+//    big primes run through the windowed bucket path of run();
+//  * direct ranges are cut into stripes of <= kStripe segments (the medium
+//    state is set up once per stripe), ordered most expensive first, and
+//    served to the persistent grid from a device counter.
+// The ranges' rows are accumulated on the device and read back once.
+#include "engine.hpp"
+#include "batch_kernel.cuh"
+#include "../../include/psgpu.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace psg {
+
+namespace {
+
+constexpr uint32_t kStripe = 8;            // segments per work item (at most)
+constexpr double kDirectBudget = 1e8;      // segments x direct primes per range
+
+#define PSG_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                 \
+      return PSG_ERR_CUDA;                                                      \
+    }                                                                           \
+  } while (0)
+
+template <typename T>
+int grow(T*& ptr, size_t& cap, size_t n, std::string& err) {
+  if (n <= cap) return PSG_OK;
+  const size_t c = std::max<size_t>(n, 2 * cap);
+  cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+  if (cudaMalloc(&ptr, c * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    err = "cannot allocate " + std::to_string(c * sizeof(T)) + " bytes of batch storage";
+    return PSG_ERR_NOMEM;
+  }
+  cap = c;
+  return PSG_OK;
+}
+
+} // namespace
+
+int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::string& err) {
+  PSG_CUDA(cudaSetDevice(device_));
+  std::fill(out, out + 6 * n, 0ull);
+  // the engine's scratch is shared with counts queued on other streams
+  if (last_stream_ && last_stream_ != stream_) PSG_CUDA(cudaStreamWaitEvent(stream_, done_event_, 0));
+  if (n == 0) return PSG_OK;
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+
+  // ---- 1. host part of every range, largest stop
+  std::vector<uint64_t> lo(n, 0), hi(n, 0);
+  std::vector<uint32_t> kinds(n, 0);
+  uint64_t max_hi = 0;
+  for (size_t i = 0; i < n; i++) {
+    const uint32_t k = q[i].kinds & 0x3fu;
+    if (q[i].start > q[i].stop || k == 0) continue;
+    uint64_t tab[6] = { 0, 0, 0, 0, 0, 0 };
+    small_table(q[i].start, q[i].stop, k, tab);
+    for (int j = 0; j < 6; j++) out[6 * i + j] += tab[j];
+    if (q[i].stop < 7) continue;
+    lo[i] = std::max<uint64_t>(q[i].start, 7);
+    hi[i] = q[i].stop;
+    kinds[i] = k;
+    max_hi = std::max(max_hi, hi[i]);
+  }
+  if (max_hi == 0) return PSG_OK;
+  int rc = ensure_primes(std::max<uint32_t>(isqrt_u64(max_hi), 7u), err);
+  if (rc) return rc;
+
+  // ---- 2. tiers and class of every range
+  const uint32_t n_small_all = count_primes_le(small_limit_, true);
+  std::vector<BatchRange> br;
+  std::vector<size_t> br_index;             // batch range -> query
+  std::vector<size_t> bucket_ranges;        // queries for the windowed path
+  std::vector<double> seg_cost;             // per batch range: cost of one segment
+  for (size_t i = 0; i < n; i++) {
+    if (!kinds[i]) continue;
+    const uint64_t seg_low0 = lo[i] - ((lo[i] - 7) % 30 + 7);
+    const uint64_t nseg = (hi[i] - 7 - seg_low0) / span + 1;
+    const uint32_t n_total = count_primes_upper(isqrt_u64(hi[i]));
+    const uint32_t n_small = std::min(n_small_all, n_total);
+    const uint32_t n_med = std::max(n_small, std::min(n_total, n_small_all + state_cap_));
+    const double direct = (double) (n_total - n_med);
+    if (direct > 0 && (direct * (double) nseg > kDirectBudget || nseg >= (1ull << 32))) {
+      bucket_ranges.push_back(i);
+      continue;
+    }
+    BatchRange r;
+    r.seg_low0 = seg_low0;
+    r.lo = lo[i];
+    r.hi = hi[i];
+    r.n_small = n_small;
+    r.n_med_end = n_med;
+    r.n_end = n_total;
+    r.kinds = kinds[i];
+    br.push_back(r);
+    br_index.push_back(i);
+    // relative cost of one segment: sieve work + one reciprocal per direct prime
+    seg_cost.push_back(1.0 + direct / 2.0e4);
+  }
+
+  // ---- 3. work items: stripes of <= kStripe segments, most expensive first
+  std::vector<BatchItem> items;
+  std::vector<double> item_cost;
+  for (size_t k = 0; k < br.size(); k++) {
+    const uint64_t nseg = (br[k].hi - 7 - br[k].seg_low0) / span + 1;
+    const uint64_t nst = (nseg + kStripe - 1) / kStripe;
+    const uint64_t len = (nseg + nst - 1) / nst;
+    for (uint64_t s0 = 0; s0 < nseg; s0 += len) {
+      BatchItem it;
+      it.range = (uint32_t) k;
+      it.seg0 = (uint32_t) s0;
+      it.nseg = (uint32_t) std::min<uint64_t>(len, nseg - s0);
+      it.pad = 0;
+      items.push_back(it);
+      item_cost.push_back(seg_cost[k] * it.nseg);
+    }
+  }
+  {
+    std::vector<uint32_t> order(items.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = (uint32_t) i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return item_cost[x] > item_cost[y]; });
+    std::vector<BatchItem> sorted(items.size());
+    for (size_t i = 0; i < order.size(); i++) sorted[i] = items[order[i]];
+    items.swap(sorted);
+  }
+  batch_direct_ranges_ = br.size();
+  batch_bucket_ranges_ = bucket_ranges.size();
+  batch_items_ = items.size();
+
+  // ---- 4. device rows: direct ranges first, then bucket ranges
+  const size_t rows = br.size() + bucket_ranges.size();
+  if ((rc = grow(d_batch_rows_, batch_rows_cap_, 6 * rows, err))) return rc;
+  if ((rc = grow(d_batch_ranges_, batch_ranges_cap_, std::max<size_t>(br.size(), 1), err))) return rc;
+  if ((rc = grow(d_batch_items_, batch_items_cap_, std::max<size_t>(items.size(), 1), err))) return rc;
+  h_batch_rows_.resize(6 * rows);
+  PSG_CUDA(cudaMemsetAsync(d_batch_rows_, 0, 6 * rows * sizeof(unsigned long long), stream_));
+  PSG_CUDA(cudaMemsetAsync(d_overflow_, 0, sizeof(uint32_t), stream_));
+
+  if (!items.empty()) {
+    PSG_CUDA(cudaMemcpyAsync(d_batch_ranges_, br.data(), br.size() * sizeof(BatchRange), cudaMemcpyHostToDevice, stream_));
+    PSG_CUDA(cudaMemcpyAsync(d_batch_items_, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, stream_));
+    PSG_CUDA(cudaMemsetAsync(d_batch_queue_, 0, sizeof(uint32_t), stream_));
+    BatchArgs b;
+    std::memset(&b, 0, sizeof b);
+    fill_common_args(b.common);
+    b.ranges = d_batch_ranges_;
+    b.items = d_batch_items_;
+    b.num_items = (uint32_t) items.size();
+    b.queue = d_batch_queue_;
+    b.counts = d_batch_rows_;
+    timed_begin(3, stream_);
+    cudaError_t e = launch_batch(b);
+    timed_end(3, stream_);
+    if (e != cudaSuccess) { err = std::string("batch kernel launch: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+  }
+  for (size_t j = 0; j < bucket_ranges.size(); j++) {
+    const size_t i = bucket_ranges[j];
+    rc = run(lo[i], hi[i], kinds[i], d_batch_rows_ + 6 * (br.size() + j), stream_, err);
+    if (rc) return rc;
+  }
+
+  // ---- 5. results
+  uint32_t overflow = 0;
+  PSG_CUDA(cudaMemcpyAsync(h_batch_rows_.data(), d_batch_rows_, 6 * rows * sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, stream_));
+  PSG_CUDA(cudaMemcpyAsync(&overflow, d_overflow_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+  PSG_CUDA(cudaStreamSynchronize(stream_));
+  for (size_t k = 0; k < br.size(); k++)
+    for (int j = 0; j < 6; j++) out[6 * br_index[k] + j] += h_batch_rows_[6 * k + j];
+  for (size_t j = 0; j < bucket_ranges.size(); j++) {
+    const size_t i = bucket_ranges[j];
+    if (overflow) {
+      // some bucket list overflowed: recount these ranges one by one
+      // (count() grows the lists until nothing overflows)
+      uint64_t c[6];
+      rc = count(lo[i], hi[i], kinds[i], c, err);
+      if (rc) return rc;
+      for (int k = 0; k < 6; k++) out[6 * i + k] += c[k];
+    } else {
+      for (int k = 0; k < 6; k++) out[6 * i + k] += h_batch_rows_[6 * (br.size() + j) + k];
+    }
+  }
+  PSG_CUDA(cudaEventRecord(done_event_, stream_));
+  last_stream_ = stream_;
+  return PSG_OK;
+}
+
+cudaError_t Engine::launch_batch(const BatchArgs& b) {
+  static_assert(sizeof(BatchArgs) < 4000, "kernel parameter space");
+  switch (block_) {
+    case 256:
+      cudaFuncSetAttribute(batch_sieve_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
+      batch_sieve_kernel<256><<<grid_, 256, smem_dyn_, stream_>>>(b);
+      break;
+    case 1024:
+      cudaFuncSetAttribute(batch_sieve_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
+      batch_sieve_kernel<1024><<<grid_, 1024, smem_dyn_, stream_>>>(b);
+      break;
+    default:
+      cudaFuncSetAttribute(batch_sieve_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
+      batch_sieve_kernel<512><<<grid_, 512, smem_dyn_, stream_>>>(b);
+      break;
+  }
+  return cudaGetLastError();
+}
+
+} // namespace psg

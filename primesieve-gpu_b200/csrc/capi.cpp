@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <cstddef>
 #include <mutex>
 #include <new>
 #include <string>
@@ -161,13 +162,14 @@ int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t ki
 
 int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n, uint64_t* counts) {
   if (!ctx || (n && (!ranges || !counts))) return fail(PSG_ERR_ARG, "NULL argument");
+  static_assert(sizeof(psg_range) == sizeof(psg::RangeQuery) &&
+                offsetof(psg_range, start) == offsetof(psg::RangeQuery, start) &&
+                offsetof(psg_range, stop) == offsetof(psg::RangeQuery, stop) &&
+                offsetof(psg_range, kinds) == offsetof(psg::RangeQuery, kinds), "psg_range layout");
   std::lock_guard<std::mutex> lock(ctx->mu);
   std::string err;
-  for (size_t i = 0; i < n; i++) {
-    int rc = ctx->engine.count(ranges[i].start, ranges[i].stop, ranges[i].kinds, counts + 6 * i, err);
-    if (rc) return fail(rc, err);
-  }
-  return PSG_OK;
+  int rc = ctx->engine.count_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, counts, err);
+  return rc ? fail(rc, err) : PSG_OK;
 }
 
 int psg_prepare(psg_context* ctx, uint64_t stop) {

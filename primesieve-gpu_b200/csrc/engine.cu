@@ -13,6 +13,26 @@
 
 namespace psg {
 
+uint32_t isqrt_u64(uint64_t x) {
+  uint64_t r = (uint64_t) std::sqrt((double) x);
+  while (r > 0 && (r > 0xffffffffull || r * r > x)) r--;
+  while (r + 1 <= 0xffffffffull && (r + 1) * (r + 1) <= x) r++;
+  return (uint32_t) r;
+}
+
+// The primes 2, 3, 5 and the k-tuplets containing them cannot be stored in
+// the wheel-30 bit array; they are counted from this table when
+// start <= 5 (reference src/gpu/GpuSieve.cpp:149-169,
+// src/PrimeSieveClass.cpp:38-48).
+void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]) {
+  struct T { uint64_t first, last; int kind; };
+  static const T tab[8] = { { 2, 2, 0 }, { 3, 3, 0 }, { 5, 5, 0 }, { 3, 5, 1 },
+                            { 5, 7, 1 }, { 5, 11, 2 }, { 5, 13, 3 }, { 5, 17, 4 } };
+  if (start > 5) return;
+  for (const T& t : tab)
+    if (((kinds >> t.kind) & 1u) && t.first >= start && t.last <= stop) out[t.kind]++;
+}
+
 namespace {
 
 constexpr int kBucketBlock = 1024;
@@ -28,17 +48,11 @@ constexpr int kSweepK = 16;         // sieving primes per sweep lane
     }                                                                           \
   } while (0)
 
-uint32_t isqrt64(uint64_t x) {
-  uint64_t r = (uint64_t) std::sqrt((double) x);
-  while (r > 0 && (r > 0xffffffffull || r * r > x)) r--;
-  while (r + 1 <= 0xffffffffull && (r + 1) * (r + 1) <= x) r++;
-  return (uint32_t) r;
-}
 
 // Primes in (after, limit], limit < 2^32, by an odd-only segmented sieve.
 void host_primes(uint32_t after, uint32_t limit, std::vector<uint32_t>& out) {
   if (limit <= after) return;
-  const uint32_t r = isqrt64(limit);
+  const uint32_t r = isqrt_u64(limit);
   std::vector<uint8_t> small(r + 1, 0);
   std::vector<uint32_t> base;
   for (uint32_t i = 3; i <= r; i += 2) {
@@ -92,18 +106,6 @@ __global__ void add_counts_kernel(unsigned long long* c, unsigned long long a0, 
   }
 }
 
-// The primes 2, 3, 5 and the k-tuplets containing them cannot be stored in
-// the wheel-30 bit array; they are counted from this table when
-// start <= 5 (reference src/gpu/GpuSieve.cpp:149-169,
-// src/PrimeSieveClass.cpp:38-48).
-void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]) {
-  struct T { uint64_t first, last; int kind; };
-  static const T tab[8] = { { 2, 2, 0 }, { 3, 3, 0 }, { 5, 5, 0 }, { 3, 5, 1 },
-                            { 5, 7, 1 }, { 5, 11, 2 }, { 5, 13, 3 }, { 5, 17, 4 } };
-  if (start > 5) return;
-  for (const T& t : tab)
-    if (((kinds >> t.kind) & 1u) && t.first >= start && t.last <= stop) out[t.kind]++;
-}
 
 template <int BLOCK>
 void set_smem_attrs(uint32_t bytes) {
@@ -200,6 +202,10 @@ Engine::~Engine() {
   cudaFree(d_overflow_);
   cudaFree(d_entry_total_);
   cudaFree(d_counts_);
+  cudaFree(d_batch_rows_);
+  cudaFree(d_batch_ranges_);
+  cudaFree(d_batch_items_);
+  cudaFree(d_batch_queue_);
   if (h_counts_) cudaFreeHost(h_counts_);
   if (done_event_) cudaEventDestroy(done_event_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -280,16 +286,20 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   big_limit_ = cfg.big_limit ? cfg.big_limit : (uint32_t) std::min<uint64_t>(span / 10u, 0xffffffffull);
   if (big_limit_ < small_limit_) big_limit_ = small_limit_;
   window_ = cfg.window_segments ? cfg.window_segments : grid_ * 8u;
-  // the bucket fill kernel scans W <= 8 * its block size segment counters
-  // and packs (segment, byte << 3 | bit) into 32 bits
-  entry_bits_ = 3;
-  while ((1u << (entry_bits_ - 3)) < seg_bytes_) entry_bits_++;
-  window_ = std::min<uint32_t>(window_, std::min<uint32_t>(8u * kBucketBlock, 1u << (32 - entry_bits_)));
   lists_ = cfg.bucket_lists ? cfg.bucket_lists : (uint32_t) prop_.multiProcessorCount;
-  // the bucket kernel indexes a window with 32-bit byte offsets
+  // the bucket fill kernel keeps one bin per window segment in shared memory
+  // and indexes a window with 32-bit byte offsets
+  const size_t fill_smem_max = (size_t) prop_.sharedMemPerBlockOptin;
+  window_ = std::min<uint32_t>(window_, (uint32_t) (fill_smem_max / fill_smem_bytes(1)));
   window_ = std::min<uint32_t>(window_, (uint32_t) ((1ull << 31) / seg_bytes_));
-  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) fill_smem_bytes<kBucketBlock>(window_));
+  window_ = std::max<uint32_t>(window_, 1u);
+  seg_pow2_ = (seg_bytes_ & (seg_bytes_ - 1u)) == 0;
+  seg_shift_ = 0;
+  while ((1u << seg_shift_) < seg_bytes_) seg_shift_++;
+  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) fill_smem_bytes(window_));
+  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) fill_smem_bytes(window_));
   cudaFuncSetAttribute(primegen_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, 131072);
   cudaFuncSetAttribute(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (window_ * sizeof(uint32_t)));
@@ -298,6 +308,7 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   sweep_limit_ = std::min<uint32_t>(cfg.sweep_limit, 120000000u);
 
   PSG_CUDA(cudaMalloc(&d_counts_, 6 * sizeof(unsigned long long)));
+  PSG_CUDA(cudaMalloc(&d_batch_queue_, sizeof(uint32_t)));
   PSG_CUDA(cudaMalloc(&d_overflow_, sizeof(uint32_t)));
   PSG_CUDA(cudaMalloc(&d_entry_total_, sizeof(unsigned long long)));
   PSG_CUDA(cudaMemset(d_entry_total_, 0, sizeof(unsigned long long)));
@@ -413,7 +424,7 @@ int Engine::ensure_primes(uint64_t limit, std::string& err) {
     const uint64_t lo = primes_upto_ + 1, hi = target;
     // base primes 7 .. sqrt(hi) (<= 2^16): the pre-sieve primes + the head
     std::vector<uint32_t> base;
-    const uint32_t r = isqrt64(hi);
+    const uint32_t r = isqrt_u64(hi);
     host_primes(6, std::min<uint32_t>(presieve_max_, r), base);
     for (uint32_t q : h_primes_) { if (q > r) break; base.push_back(q); }
     uint32_t n_small = 0;
@@ -478,6 +489,17 @@ int Engine::ensure_primes(uint64_t limit, std::string& err) {
     cudaFree(d_s);
     if (e != cudaSuccess) { err = std::string("prime sample: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
   }
+  // prefix of sum(1/p) per sample block: exact inside the host head, the
+  // block's first (smallest) prime for all of a block beyond it (an upper
+  // bound, which is what the bucket capacities need)
+  h_inv_block_.assign(ns + 1, 0.0);
+  for (size_t k = 0; k < ns; k++) {
+    const size_t j0 = k * kSample, j1 = std::min<size_t>(j0 + kSample, n_dev_);
+    const size_t jh = std::min(std::max(j0, h_primes_.size()), j1);   // [j0, jh) in the head
+    double v = (double) (j1 - jh) / (double) h_sample_[k];
+    for (size_t j = j0; j < jh; j++) v += 1.0 / (double) h_primes_[j];
+    h_inv_block_[k + 1] = h_inv_block_[k] + v;
+  }
   return PSG_OK;
 }
 
@@ -502,6 +524,27 @@ uint32_t Engine::count_primes_le(uint64_t v, bool strict) {
   return (uint32_t) (b0 + (size_t) (jt - blk));
 }
 
+// An upper bound of the number of table primes <= v from the host tables
+// alone: exact inside the head, the end of v's sample block beyond it.
+uint32_t Engine::count_primes_upper(uint64_t v) const {
+  const uint32_t x = (uint32_t) std::min<uint64_t>(v, 0xffffffffull);
+  if (!h_primes_.empty() && (x < h_primes_.back() || n_dev_ == h_primes_.size()))
+    return (uint32_t) (std::upper_bound(h_primes_.begin(), h_primes_.end(), x) - h_primes_.begin());
+  const size_t k = (size_t) (std::upper_bound(h_sample_.begin(), h_sample_.end(), x) - h_sample_.begin());
+  return (uint32_t) std::min<size_t>(std::max<size_t>(k * kSample, h_primes_.size()), n_dev_);
+}
+
+// Number of table primes < v from the host tables alone: exact inside the
+// head, rounded to a sample block beyond it (for splits that only steer
+// work, never correctness).
+uint32_t Engine::approx_count_below(uint64_t v) const {
+  const uint32_t x = (uint32_t) std::min<uint64_t>(v, 0xffffffffull);
+  if (!h_primes_.empty() && x <= h_primes_.back())
+    return (uint32_t) (std::lower_bound(h_primes_.begin(), h_primes_.end(), x) - h_primes_.begin());
+  const size_t k = (size_t) (std::lower_bound(h_sample_.begin(), h_sample_.end(), x) - h_sample_.begin());
+  return (uint32_t) std::min<size_t>(std::max<size_t>(k * kSample, h_primes_.size()), n_dev_);
+}
+
 // Table prime i for planning: exact in the host head, else the smallest prime
 // of its sample block (a slight underestimate).
 double Engine::approx_prime(uint32_t i) const {
@@ -509,9 +552,18 @@ double Engine::approx_prime(uint32_t i) const {
   return (double) h_sample_[std::min<size_t>(i / kSample, h_sample_.size() - 1)];
 }
 
+// Sum of 1/p over table primes [0, i), same weights as h_inv_block_.
+double Engine::inv_prefix(uint32_t i) const {
+  const size_t k = i / kSample;
+  double v = h_inv_block_[std::min(k, h_inv_block_.size() - 1)];
+  for (size_t j = k * kSample; j < i; j++)
+    v += 1.0 / (double) (j < h_primes_.size() ? h_primes_[j] : h_sample_[k]);
+  return v;
+}
+
 int Engine::prepare(uint64_t stop, std::string& err) {
   PSG_CUDA(cudaSetDevice(device_));
-  return ensure_primes(std::max<uint32_t>(isqrt64(stop), 7u), err);
+  return ensure_primes(std::max<uint32_t>(isqrt_u64(stop), 7u), err);
 }
 
 // Bucket lists for the big primes primes[first, last):
@@ -558,39 +610,25 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
   if (nfill) {
     fill_ctas = std::max<uint32_t>(1, std::min<uint32_t>(lists_, nfill));
     const double win_span = span * (8.0 / 30.0) * (double) window_;
-    const double setup = 8.0;
-    // pieces [i0, i1) with their sum of 1/p: single primes inside the exact
-    // host head, whole sample blocks beyond it
-    std::vector<uint32_t> pc_begin;
-    std::vector<double> pc_inv;
-    for (uint32_t i = mid; i < last;) {
-      uint32_t j;
-      double inv;
-      if (i < h_primes_.size()) { j = i + 1; inv = 1.0 / (double) h_primes_[i]; }
-      else {
-        j = std::min<uint32_t>(last, (uint32_t) ((i / kSample + 1) * kSample));
-        inv = (double) (j - i) / approx_prime(i);
-      }
-      pc_begin.push_back(i);
-      pc_inv.push_back(inv);
-      i = j;
-    }
-    pc_begin.push_back(last);
-    double total = 0;
-    for (size_t q = 0; q + 1 < pc_begin.size(); q++)
-      total += setup * (pc_begin[q + 1] - pc_begin[q]) + win_span * pc_inv[q];
+    const double setup = 8.0;      // per-window setup of a prime, in entries
+    // chunk boundaries for equal (setup + hits) work: binary search on the
+    // monotone cost over the 1/p prefix table
+    const double s_mid = inv_prefix(mid);
+    const auto cost = [&](uint32_t i) { return setup * (double) (i - mid) + win_span * (inv_prefix(i) - s_mid); };
+    const double total = cost(last);
     begin.assign(fill_ctas + 1, last);
     begin[0] = mid;
-    std::vector<double> mu(fill_ctas, 0.0);
-    double acc = 0;
-    uint32_t l = 1;
-    for (size_t q = 0; q + 1 < pc_begin.size(); q++) {
-      mu[l - 1] += per_seg * pc_inv[q];
-      acc += setup * (pc_begin[q + 1] - pc_begin[q]) + win_span * pc_inv[q];
-      if (l < fill_ctas && acc >= total * (double) l / (double) fill_ctas) begin[l++] = pc_begin[q + 1];
+    for (uint32_t l = 1; l < fill_ctas; l++) {
+      const double target = total * (double) l / (double) fill_ctas;
+      uint32_t x = begin[l - 1], y = last;       // smallest i in [x, y] with cost(i) >= target
+      while (x < y) {
+        const uint32_t m = x + (y - x) / 2;
+        if (cost(m) >= target) y = m; else x = m + 1;
+      }
+      begin[l] = x;
     }
-    for (; l < fill_ctas; l++) begin[l] = last;
-    begin[fill_ctas] = last;
+    std::vector<double> mu(fill_ctas, 0.0);
+    for (uint32_t c = 0; c < fill_ctas; c++) mu[c] = per_seg * (inv_prefix(begin[c + 1]) - inv_prefix(begin[c]));
     for (uint32_t c = 0; c < fill_ctas; c++) add_list(mu[c]);
   }
   const uint32_t lists = sweep_ctas + fill_ctas;
@@ -678,34 +716,10 @@ void Engine::reset_kernel_stats() {
   for (auto& t : timed_) { t.launches = 0; t.ms = 0; }
 }
 
-int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
-                cudaStream_t st, std::string& err) {
-  // lo >= 7, lo <= hi
-  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
-  // byteRemainder (reference src/Erat.cpp:231-237, CudaBackend.cpp:457)
-  const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
-  const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
-  const uint32_t sq = isqrt64(hi);
-  int rc = ensure_primes(std::max<uint32_t>(sq, 7u), err);
-  if (rc) return rc;
-
-  const auto upto = [&](uint64_t v) { return count_primes_le(v, false); };
-  const auto below = [&](uint64_t v) { return count_primes_le(v, true); };
-  const uint32_t n_total = upto(sq);
-  const uint32_t n_small = std::min(below(small_limit_), n_total);
-  // medium primes must fit the shared-memory state area; the rest go to buckets
-  const uint32_t n_med = std::max(n_small, std::min({ below(big_limit_), n_total, n_small + state_cap_ }));
-  const bool use_buckets = n_med < n_total;
-  // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
-  const uint32_t n_sweep_end = std::max(n_med, std::min(below(sweep_limit_), n_total));
-  if (use_buckets) {
-    rc = ensure_buckets(n_med, n_sweep_end, n_total, err);
-    if (rc) return rc;
-  }
-
-  SieveArgs a;
+// Launch-wide sieve arguments: segment size, pre-sieve tables, sieving
+// primes and the wheel walk tables (range and tier fields zero).
+void Engine::fill_common_args(SieveArgs& a) const {
   std::memset(&a, 0, sizeof a);
-  a.lo = lo; a.hi = hi;
   a.seg_bytes = seg_bytes_;
   a.num_tables = (uint32_t) pat_period_.size();
   for (size_t t = 0; t < pat_period_.size(); t++) {
@@ -720,12 +734,45 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
   a.presieve_max = presieve_max_;
   a.primes = d_primes_;
   a.recip = d_recip_;
-  a.n_small = n_small;
-  a.n_primes = n_med;
   for (uint32_t c = 0; c < 8; c++) {
     a.wheel_tab[2 * c] = wheel_bits_packed(c);
     a.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
   }
+}
+
+int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
+                cudaStream_t st, std::string& err) {
+  // lo >= 7, lo <= hi
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  // byteRemainder (reference src/Erat.cpp:231-237, CudaBackend.cpp:457)
+  const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
+  const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
+  const uint32_t sq = isqrt_u64(hi);
+  int rc = ensure_primes(std::max<uint32_t>(sq, 7u), err);
+  if (rc) return rc;
+
+  const auto upto = [&](uint64_t v) { return count_primes_le(v, false); };
+  const auto below = [&](uint64_t v) { return count_primes_le(v, true); };
+  const uint32_t n_total = upto(sq);
+  const uint32_t n_small = std::min(below(small_limit_), n_total);
+  // medium primes must fit the shared-memory state area; the rest go to buckets
+  const uint32_t n_med = std::max(n_small, std::min({ below(big_limit_), n_total, n_small + state_cap_ }));
+  // beyond the shared state and below big_limit_: direct tier (no state)
+  const uint32_t n_dir = std::max(n_med, std::min(below(big_limit_), n_total));
+  const bool use_buckets = n_dir < n_total;
+  // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
+  const uint32_t n_sweep_end = std::max(n_dir, std::min(below(sweep_limit_), n_total));
+  if (use_buckets) {
+    rc = ensure_buckets(n_dir, n_sweep_end, n_total, err);
+    if (rc) return rc;
+  }
+
+  SieveArgs a;
+  fill_common_args(a);
+  a.lo = lo; a.hi = hi;
+  a.n_small = n_small;
+  a.n_primes = n_med;
+  a.n_direct = n_dir;
   a.kinds = kinds;
   a.counts = dev_counts;
   const bool all = (kinds & ~1u) != 0;
@@ -777,7 +824,9 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
         b.win_segments = (uint32_t) ns;
         b.seg_bytes = seg_bytes_;
         b.seg_magic = (uint32_t) ((1ull << 32) / seg_bytes_ + 1u);
-        b.entry_bits = entry_bits_;
+        b.seg_shift = seg_shift_;
+        // steps per tile: a bin expects at most ~45% of its slots per tile
+        b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (0.45 * kBinCap * (double) ns / kBucketBlock));
         b.primes = d_primes_;
         b.recip = d_recip_;
         b.chunk_begin = d_chunk_begin_;
@@ -791,8 +840,10 @@ int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* de
         b.overflow = d_overflow_;
         b.entry_total = d_entry_total_;
         timed_begin(1, st);
-        bucket_fill_kernel<kBucketBlock>
-            <<<fill_ctas_, kBucketBlock, fill_smem_bytes<kBucketBlock>((uint32_t) ns), st>>>(b);
+        if (seg_pow2_)
+          bucket_fill_kernel<kBucketBlock, true><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), st>>>(b);
+        else
+          bucket_fill_kernel<kBucketBlock, false><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), st>>>(b);
         timed_end(1, st);
         PSG_CUDA(cudaGetLastError());
       }

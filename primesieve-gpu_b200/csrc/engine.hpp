@@ -28,6 +28,23 @@ struct EngineConfig {
   uint32_t sweep_limit = 0;      // big primes below: segment-major sweep; 0 = auto
 };
 
+// One range of a batch; same layout as psg_range (include/psgpu.h).
+struct RangeQuery {
+  uint64_t start, stop;
+  uint32_t kinds, reserved;
+};
+
+struct SieveArgs;
+struct BatchArgs;
+struct BatchRange;
+struct BatchItem;
+
+// floor(sqrt(x))
+uint32_t isqrt_u64(uint64_t x);
+// The primes 2, 3, 5 and the k-tuplets containing them (not representable
+// in the wheel-30 bit array): counts added to out[kind] when start <= 5.
+void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]);
+
 struct KernelStat {
   const char* name;
   uint64_t launches = 0;
@@ -52,6 +69,15 @@ public:
 
   // Synchronous host-result version (counts[6] overwritten).
   int count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6], std::string& err);
+
+  // Count n ranges (out is n x 6, row i for q[i]) with the persistent batch
+  // kernel; ranges that need the bucket tier run through the range path.
+  int count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::string& err);
+  // Classes of the last batch: ranges in the persistent kernel, ranges on
+  // the windowed bucket path, work items.
+  size_t batch_direct_ranges() const { return batch_direct_ranges_; }
+  size_t batch_bucket_ranges() const { return batch_bucket_ranges_; }
+  size_t batch_items() const { return batch_items_; }
 
   // Make sure the sieving-prime table covers sqrt(stop) (host work + upload).
   int prepare(uint64_t stop, std::string& err);
@@ -82,7 +108,12 @@ private:
   int ensure_primes(uint64_t limit, std::string& err);
   int reserve_primes(size_t n, size_t keep, std::string& err);
   uint32_t count_primes_le(uint64_t v, bool strict);
+  uint32_t count_primes_upper(uint64_t v) const;   // >= table primes <= v, no device read
+  void fill_common_args(SieveArgs& a) const;
+  cudaError_t launch_batch(const BatchArgs& b);
   double approx_prime(uint32_t i) const;
+  double inv_prefix(uint32_t i) const;   // ~ sum of 1/p over table primes [0, i)
+  uint32_t approx_count_below(uint64_t v) const;
   int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
@@ -99,7 +130,8 @@ private:
   EngineConfig cfg_;
   uint32_t seg_bytes_ = 0, block_ = 0, grid_ = 0, bucket_block_ = 256;
   uint32_t small_limit_ = 0, big_limit_ = 0, window_ = 0, lists_ = 0;
-  uint32_t state_cap_ = 0, smem_dyn_ = 0, entry_bits_ = 20;
+  uint32_t state_cap_ = 0, smem_dyn_ = 0, seg_shift_ = 0;
+  bool seg_pow2_ = true;
 
   // pre-sieve tables
   std::vector<std::vector<uint32_t>> groups_;
@@ -115,6 +147,7 @@ private:
   static constexpr size_t kSample = 256;
   std::vector<uint32_t> h_primes_;
   std::vector<uint32_t> h_sample_;
+  std::vector<double> h_inv_block_;      // [blocks + 1] prefix of sum(1/p) per sample block
   size_t n_dev_ = 0;
   uint64_t primes_upto_ = 0;
   uint32_t* d_primes_ = nullptr;
@@ -144,12 +177,23 @@ private:
   unsigned long long* d_counts_ = nullptr;
   unsigned long long* h_counts_ = nullptr;   // pinned
 
+  // batch storage
+  unsigned long long* d_batch_rows_ = nullptr;
+  size_t batch_rows_cap_ = 0;
+  BatchRange* d_batch_ranges_ = nullptr;
+  size_t batch_ranges_cap_ = 0;
+  BatchItem* d_batch_items_ = nullptr;
+  size_t batch_items_cap_ = 0;
+  uint32_t* d_batch_queue_ = nullptr;
+  std::vector<unsigned long long> h_batch_rows_;
+  size_t batch_direct_ranges_ = 0, batch_bucket_ranges_ = 0, batch_items_ = 0;
+
   // profiling
   bool profiling_ = false;
   // launches are always counted; CUDA-event times only while profiling
   struct Timed { const char* name; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev; uint64_t launches = 0; double ms = 0; };
-  Timed timed_[3] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 },
-                      { "bucket_sweep_kernel", {}, 0, 0 } };
+  Timed timed_[4] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 },
+                      { "bucket_sweep_kernel", {}, 0, 0 }, { "batch_sieve_kernel", {}, 0, 0 } };
 };
 
 } // namespace psg

@@ -56,6 +56,8 @@ struct SieveArgs {
   uint32_t n_small;           // primes[0, n_small): warp-cooperative
   uint32_t n_primes;          // primes[n_small, n_primes): thread per prime
                               // (their state fits the shared-memory area)
+  uint32_t n_direct;          // primes[n_primes, n_direct): thread per prime,
+                              // first multiple recomputed every segment
   // big primes via buckets (num_bucket_lists == 0: none)
   const uint32_t* bucket_entries;   // [segment][seg_stride] entries
   const uint32_t* bucket_counts;    // [segment][list] number of entries
@@ -137,6 +139,335 @@ __device__ __forceinline__ void count_word(uint32_t w, uint32_t (&c)[6]) {
   }
 }
 
+// ---- per-segment phases ---------------------------------------------------
+// Shared by the range kernel below and the batch kernel (batch_kernel.cuh).
+// `a` carries what is common to a launch (tables, sieving primes, segment
+// size); prime-tier bounds, segment base and range edges are arguments.
+
+constexpr int kSmallRegs = 2;                // small primes per lane kept in registers
+constexpr uint32_t kMedFar = 0xffffffffu;  // medium state: next multiple not representable yet
+
+// 1. pre-sieve: AND of the pattern tables, 16 bytes per thread per step.
+template <int BLOCK>
+__device__ __forceinline__ void phase_presieve(const SieveArgs& a, uint4* smem4, uint64_t segLow, uint32_t tid) {
+  const uint32_t nchunks = a.seg_bytes >> 4;
+  const uint64_t g0 = segLow / 30u;   // global byte index of byte 0
+  uint32_t phase[kMaxPresieveTables], step[kMaxPresieveTables];
+#pragma unroll
+  for (int t = 0; t < kMaxPresieveTables; t++) {
+    if (t < (int) a.num_tables) {
+      const uint32_t P = a.pat_period[t];
+      phase[t] = mod_recip(g0 + 16ull * tid, P, a.pat_rcp[t]);
+      step[t] = (16u * BLOCK) % P;
+    }
+  }
+  for (uint32_t c = tid; c < nchunks; c += BLOCK) {
+    uint4 v = make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+    for (int t = 0; t < kMaxPresieveTables; t++) {
+      if (t < (int) a.num_tables) {
+        const uint32_t ph = phase[t];
+        const uint32_t k = ph & 15u;
+        const uint4 pv = __ldg(reinterpret_cast<const uint4*>(
+            a.pat_base[t] + (size_t) k * a.pat_stride[t] + (ph - k)));
+        v.x &= pv.x; v.y &= pv.y; v.z &= pv.z; v.w &= pv.w;
+        uint32_t np = ph + step[t];
+        phase[t] = (np >= a.pat_period[t]) ? np - a.pat_period[t] : np;
+      }
+    }
+    if (c == 0 && segLow <= a.presieve_max) {
+      // The patterns also cleared the pre-sieve primes themselves;
+      // put them back (reference: restore bytes, GpuTables.cpp:108-127).
+      uint32_t w4[4] = { v.x, v.y, v.z, v.w };
+      for (uint32_t i = 0; i < a.num_presieve_primes; i++) {
+        const uint64_t q = a.presieve_primes[i];
+        if (q < segLow + 7) continue;
+        const uint64_t rel = q - segLow - 7;      // < 16*30
+        const uint32_t byte = (uint32_t) (rel / 30u);
+        if (byte >= 16) continue;
+        const uint32_t bit = residue_to_bit((uint32_t) (q % 30u));
+        w4[byte >> 2] |= 1u << (8 * (byte & 3) + bit);
+      }
+      v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
+    smem4[c] = v;
+  }
+}
+
+// Small primes of this warp, register resident: p, r = (segLow+7) mod p of
+// the current segment, and span mod p to advance r by one segment.
+template <int BLOCK>
+__device__ __forceinline__ void small_setup(const SieveArgs& a, uint32_t n_small, uint64_t x0, bool active,
+                                            uint32_t warp, uint32_t lane, uint32_t (&sp)[kSmallRegs],
+                                            uint32_t (&sr)[kSmallRegs], uint32_t (&sdl)[kSmallRegs]) {
+  constexpr uint32_t NWARPS = BLOCK / 32;
+  const uint64_t span = (uint64_t) a.seg_bytes * 30u;
+#pragma unroll
+  for (int m = 0; m < kSmallRegs; m++) {
+    const uint32_t idx = warp + NWARPS * (lane + 32u * m);
+    sp[m] = 1; sr[m] = 0; sdl[m] = 0;
+    if (idx < n_small && active) {
+      const uint32_t p = a.primes[idx];
+      sp[m] = p;
+      sr[m] = mod_recip(x0, p, a.recip[idx]);
+      sdl[m] = (uint32_t) (span % p);
+    }
+  }
+}
+
+__device__ __forceinline__ void small_advance(uint32_t (&sp)[kSmallRegs], uint32_t (&sr)[kSmallRegs],
+                                              const uint32_t (&sdl)[kSmallRegs]) {
+#pragma unroll
+  for (int m = 0; m < kSmallRegs; m++) {
+    const uint32_t nr = sr[m] + sdl[m];
+    sr[m] = (nr >= sp[m]) ? nr - sp[m] : nr;
+  }
+}
+
+// 2. small primes: one warp per prime; lane (j = lane&7, r = lane>>3) walks
+// the multiples with cofactor class j, every 4th from phase r (stride p words).
+template <int BLOCK>
+__device__ __forceinline__ void phase_small(const SieveArgs& a, uint32_t n_small, uint32_t* sieve32, uint64_t segLow,
+                                            uint32_t warp, uint32_t lane, const uint32_t (&sp)[kSmallRegs],
+                                            const uint32_t (&sr)[kSmallRegs]) {
+  constexpr uint32_t NWARPS = BLOCK / 32;
+  const uint32_t seg_bytes = a.seg_bytes;
+  const uint32_t nwords = seg_bytes >> 2;
+  const uint64_t span = (uint64_t) seg_bytes * 30u;
+  const uint32_t j = lane & 7u;
+  const uint32_t r = lane >> 3;
+  const uint32_t Q = cofactor_class(j);
+  const uint64_t x0 = segLow + 7;
+#pragma unroll
+  for (int m = 0; m < kSmallRegs; m++) {
+    const uint32_t tbase = 32u * m;
+    if (warp + NWARPS * tbase >= n_small) break;
+    for (uint32_t l = 0; l < 32; l++) {
+      const uint32_t idx = warp + NWARPS * (tbase + l);
+      if (idx >= n_small) break;
+      const uint32_t p = __shfl_sync(0xffffffffu, sp[m], l);
+      const uint32_t rem = __shfl_sync(0xffffffffu, sr[m], l);
+      const uint32_t pm = p % 30u;
+      const uint64_t pp = (uint64_t) p * p;
+      uint64_t d; uint32_t c0;
+      if (x0 <= pp) {
+        d = pp - x0;
+        c0 = pm;
+        if (d >= span) continue;
+      } else {
+        const uint32_t dd = rem ? p - rem : 0u;
+        d = dd;
+        c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
+      }
+      const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+      const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
+      if (b64 < seg_bytes) {
+        const uint32_t b = (uint32_t) b64;
+        const uint32_t bit = residue_to_bit((Q * pm) % 30u);
+        const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
+        for (uint32_t w = b >> 2; w < nwords; w += p)
+          atomicAnd(&sieve32[w], mask);
+      }
+    }
+  }
+  // small primes beyond the register-resident ones
+  for (uint32_t idx = warp + NWARPS * 32u * kSmallRegs; idx < n_small; idx += NWARPS) {
+    const uint32_t p = a.primes[idx];
+    uint64_t d; uint32_t c0;
+    first_multiple(segLow, p, a.recip[idx], d, c0);
+    if (d >= span) continue;
+    const uint32_t pm = p % 30u;
+    const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+    const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
+    if (b64 < seg_bytes) {
+      const uint32_t b = (uint32_t) b64;
+      const uint32_t bit = residue_to_bit((Q * pm) % 30u);
+      const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
+      for (uint32_t w = b >> 2; w < nwords; w += p)
+        atomicAnd(&sieve32[w], mask);
+    }
+  }
+}
+
+// Medium primes primes[first, first + n): state (byte << 3 | wheel index)
+// relative to the current segment, or kMedFar when the first multiple is
+// still far away.
+__device__ __forceinline__ uint32_t medium_state(uint64_t segLow, uint32_t p, uint64_t rcp) {
+  uint64_t d; uint32_t c0;
+  first_multiple(segLow, p, rcp, d, c0);
+  const uint32_t j = first_class_ge(c0);
+  const uint64_t b = (d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u;
+  return (b < (1ull << 29) - 1) ? (uint32_t) (b << 3) | j : kMedFar;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void medium_setup(const SieveArgs& a, uint32_t first, uint32_t n, uint32_t* mstate,
+                                             uint64_t segLow, uint32_t tid) {
+  for (uint32_t i = tid; i < n; i += BLOCK)
+    mstate[i] = medium_state(segLow, a.primes[first + i], a.recip[first + i]);
+}
+
+// One prime's sequential wheel walk from byte b (wheel index j) to the end
+// of the segment; returns the byte past the segment where it stopped.
+__device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t* wheel_tab, uint32_t p,
+                                               uint32_t b, uint32_t& j, uint32_t seg_bytes) {
+  const uint32_t pdiv30 = p / 30u;
+  const uint32_t cls = residue_to_bit(p - 30u * pdiv30);
+  const uint32_t bits = wheel_tab[2 * cls];
+  const uint32_t corr = wheel_tab[2 * cls + 1];
+  do {
+    const uint32_t sh = 3u * j;
+    atomicAnd(&sieve32[b >> 2], ~(1u << (((bits >> sh) & 7u) + 8u * (b & 3u))));
+    b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
+    j = (j + 1u) & 7u;
+  } while (b < seg_bytes);
+  return b;
+}
+
+// 3. medium primes: one thread per prime, carried wheel walk.
+template <int BLOCK>
+__device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first, uint32_t n, uint32_t* mstate,
+                                             uint32_t* sieve32, const uint32_t* wheel_tab, uint64_t segLow,
+                                             uint32_t tid) {
+  const uint32_t seg_bytes = a.seg_bytes;
+  uint32_t i = tid;
+  uint32_t p = 0;
+  if (i < n) p = a.primes[first + i];
+  for (; i < n; i += BLOCK) {
+    const uint32_t inext = i + BLOCK;
+    const uint32_t pn = (inext < n) ? a.primes[first + inext] : 0u;
+    uint32_t st = mstate[i];
+    if (st == kMedFar) st = medium_state(segLow, p, a.recip[first + i]);
+    if (st != kMedFar) {
+      uint32_t b = st >> 3;
+      uint32_t j = st & 7u;
+      if (b < seg_bytes) b = wheel_walk(sieve32, wheel_tab, p, b, j, seg_bytes);
+      const uint32_t nb = b - seg_bytes;
+      st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kMedFar;
+    }
+    mstate[i] = st;
+    p = pn;
+  }
+}
+
+// 3b. direct primes primes[first, end): one thread per prime, no carried
+// state. Beyond what the shared state holds, a prime that still hits most
+// segments is cheaper to locate again (one reciprocal multiply) than to
+// route through the bucket lists.
+template <int BLOCK>
+__device__ __forceinline__ void phase_direct(const SieveArgs& a, uint32_t first, uint32_t end, uint32_t* sieve32,
+                                             const uint32_t* wheel_tab, uint64_t segLow, uint32_t tid) {
+  constexpr uint32_t kDU = 4;         // primes in flight per thread
+  const uint32_t seg_bytes = a.seg_bytes;
+  const uint64_t span = (uint64_t) seg_bytes * 30u;
+  for (uint32_t i0 = first + tid; i0 < end; i0 += kDU * BLOCK) {
+    uint32_t pv[kDU];
+    uint64_t rv[kDU];
+#pragma unroll
+    for (uint32_t u = 0; u < kDU; u++) {
+      const uint32_t i = i0 + u * BLOCK;
+      pv[u] = (i < end) ? a.primes[i] : 0u;
+      rv[u] = (i < end) ? a.recip[i] : 0ull;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kDU; u++) {
+      const uint32_t p = pv[u];
+      if (p == 0) continue;
+      uint64_t d; uint32_t c0;
+      first_multiple(segLow, p, rv[u], d, c0);
+      if (d >= span) continue;
+      uint32_t j = first_class_ge(c0);
+      const uint32_t b = (uint32_t) ((d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u);
+      if (b >= seg_bytes) continue;
+      wheel_walk(sieve32, wheel_tab, p, b, j, seg_bytes);
+    }
+  }
+}
+
+// 4. big primes: the bucket lists of launch segment s. Warps take lists from
+// a shared counter (lists differ in length); each lane applies 4 entries per
+// 16-byte load (lists start 16-byte aligned).
+__device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, uint32_t* sieve32,
+                                              uint32_t* list_next, uint32_t lane) {
+  const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
+  const uint32_t* seg_entries = a.bucket_entries + s * a.bucket_seg_stride;
+  for (;;) {
+    uint32_t l = 0;
+    if (lane == 0) l = atomicAdd(list_next, 1u);
+    l = __shfl_sync(0xffffffffu, l, 0);
+    if (l >= a.num_bucket_lists) break;
+    const uint32_t n = cnt[l];
+    const uint32_t* e = seg_entries + a.bucket_list_off[l];
+    const uint32_t n4 = n & ~3u;
+    for (uint32_t x = 4 * lane; x < n4; x += 128) {
+      const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(e + x));
+      const uint32_t v[4] = { v4.x, v4.y, v4.z, v4.w };
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint32_t bb = v[q] >> 3;       // entry: byte index << 3 | bit
+        atomicAnd(&sieve32[bb >> 2], ~(1u << ((v[q] & 7u) + 8u * (bb & 3u))));
+      }
+    }
+    if (n4 + lane < n) {
+      const uint32_t v = __ldg(e + n4 + lane);
+      const uint32_t bb = v >> 3;
+      atomicAnd(&sieve32[bb >> 2], ~(1u << ((v & 7u) + 8u * (bb & 3u))));
+    }
+  }
+}
+
+// 5. mask the range edges [lo, hi] and count into acc.
+template <int BLOCK, bool ALL_KINDS>
+__device__ __forceinline__ void phase_count(const uint4* smem4, uint32_t seg_bytes, uint64_t segLow,
+                                            uint64_t lo, uint64_t hi, uint32_t tid, uint64_t (&acc)[6]) {
+  const uint32_t nchunks = seg_bytes >> 4;
+  const uint64_t span = (uint64_t) seg_bytes * 30u;
+  const uint64_t rhi = hi - segLow;                   // >= 7
+  const uint64_t rlo = (lo > segLow) ? lo - segLow : 0;
+  const bool full = (rlo <= 7) && (rhi >= span + 1);
+  uint32_t c[6] = { 0, 0, 0, 0, 0, 0 };
+  for (uint32_t ch = tid; ch < nchunks; ch += BLOCK) {
+    uint4 v = smem4[ch];
+    if (!full) {
+      uint32_t w4[4] = { v.x, v.y, v.z, v.w };
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        uint32_t m = 0;
+#pragma unroll
+        for (int by = 0; by < 4; by++) {
+          const uint64_t base = 30ull * (16ull * ch + 4u * q + by);
+          m |= byte_keep(base, rlo, rhi) << (8 * by);
+        }
+        w4[q] &= m;
+      }
+      v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
+    count_word<ALL_KINDS>(v.x, c);
+    count_word<ALL_KINDS>(v.y, c);
+    count_word<ALL_KINDS>(v.z, c);
+    count_word<ALL_KINDS>(v.w, c);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; k++) acc[k] += c[k];
+}
+
+// Warp reduction of acc, one 64-bit atomic per warp and requested kind.
+template <bool ALL_KINDS>
+__device__ __forceinline__ void flush_counts(uint64_t (&acc)[6], uint32_t kinds, unsigned long long* out,
+                                             uint32_t lane) {
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    if (!ALL_KINDS && k > 0) break;
+    uint64_t v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && v && ((kinds >> k) & 1u))
+      atomicAdd(&out[k], (unsigned long long) v);
+    acc[k] = 0;
+  }
+}
+
+// ---- the range kernel: one range, persistent grid of segment stripes -------
 template <int BLOCK, bool ALL_KINDS>
 __global__ void __launch_bounds__(BLOCK)
 sieve_count_kernel(const __grid_constant__ SieveArgs a)
@@ -144,16 +475,10 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
   extern __shared__ uint4 smem4[];
   uint32_t* const sieve32 = reinterpret_cast<uint32_t*>(smem4);
   uint32_t* const mstate = sieve32 + (a.seg_bytes >> 2);   // medium-prime state
-  constexpr int NWARPS = BLOCK / 32;
-  constexpr int SREG = 2;
-  constexpr uint32_t kFar = 0xffffffffu;   // state: next multiple not representable yet
   const uint32_t tid = threadIdx.x;
   const uint32_t lane = tid & 31u;
   const uint32_t warp = tid >> 5;
-  const uint32_t seg_bytes = a.seg_bytes;
-  const uint32_t nchunks = seg_bytes >> 4;
-  const uint32_t nwords = seg_bytes >> 2;
-  const uint64_t span = (uint64_t) seg_bytes * 30u;
+  const uint64_t span = (uint64_t) a.seg_bytes * 30u;
   const uint32_t n_med = a.n_primes - a.n_small;
 
   // contiguous stripe of segments
@@ -167,267 +492,25 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
   __shared__ uint32_t list_next;           // bucket list dispenser (per segment)
   if (tid < 16) wheel_tab[tid] = a.wheel_tab[tid];
 
-  // small primes of this warp, register resident: p, r = (segLow+7) mod p of
-  // the current segment, and span mod p to advance r by one segment.
-  uint32_t sp[SREG], sr[SREG], sdl[SREG];
-  {
-    const uint64_t x0 = a.seg_low0 + s_begin * span + 7;
-#pragma unroll
-    for (int m = 0; m < SREG; m++) {
-      const uint32_t idx = warp + NWARPS * (lane + 32u * m);
-      sp[m] = 1; sr[m] = 0; sdl[m] = 0;
-      if (idx < a.n_small && s_begin < s_end) {
-        const uint32_t p = a.primes[idx];
-        sp[m] = p;
-        sr[m] = mod_recip(x0, p, a.recip[idx]);
-        sdl[m] = (uint32_t) (span % p);
-      }
-    }
-  }
-
-  // medium primes: state (byte << 3 | wheel index) relative to the stripe's
-  // current segment, or kFar when the first multiple is still far away.
-  if (s_begin < s_end) {
-    const uint64_t segLow = a.seg_low0 + s_begin * span;
-    for (uint32_t i = tid; i < n_med; i += BLOCK) {
-      const uint32_t p = a.primes[a.n_small + i];
-      uint64_t d; uint32_t c0;
-      first_multiple(segLow, p, a.recip[a.n_small + i], d, c0);
-      const uint32_t j = first_class_ge(c0);
-      const uint64_t b = (d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u;
-      mstate[i] = (b < (1ull << 29) - 1) ? (uint32_t) (b << 3) | j : kFar;
-    }
-  }
+  uint32_t sp[kSmallRegs], sr[kSmallRegs], sdl[kSmallRegs];
+  small_setup<BLOCK>(a, a.n_small, a.seg_low0 + s_begin * span + 7, s_begin < s_end, warp, lane, sp, sr, sdl);
+  if (s_begin < s_end) medium_setup<BLOCK>(a, a.n_small, n_med, mstate, a.seg_low0 + s_begin * span, tid);
 
   for (uint64_t s = s_begin; s < s_end; s++) {
     const uint64_t segLow = a.seg_low0 + s * span;
     if (tid == 0) list_next = 0;      // read after the next barrier
-
-    // ---- 1. pre-sieve --------------------------------------------------
-    {
-      const uint64_t g0 = segLow / 30u;   // global byte index of byte 0
-      uint32_t phase[kMaxPresieveTables], step[kMaxPresieveTables];
-#pragma unroll
-      for (int t = 0; t < kMaxPresieveTables; t++) {
-        if (t < (int) a.num_tables) {
-          const uint32_t P = a.pat_period[t];
-          phase[t] = mod_recip(g0 + 16ull * tid, P, a.pat_rcp[t]);
-          step[t] = (16u * BLOCK) % P;
-        }
-      }
-      for (uint32_t c = tid; c < nchunks; c += BLOCK) {
-        uint4 v = make_uint4(~0u, ~0u, ~0u, ~0u);
-#pragma unroll
-        for (int t = 0; t < kMaxPresieveTables; t++) {
-          if (t < (int) a.num_tables) {
-            const uint32_t ph = phase[t];
-            const uint32_t k = ph & 15u;
-            const uint4 pv = __ldg(reinterpret_cast<const uint4*>(
-                a.pat_base[t] + (size_t) k * a.pat_stride[t] + (ph - k)));
-            v.x &= pv.x; v.y &= pv.y; v.z &= pv.z; v.w &= pv.w;
-            uint32_t np = ph + step[t];
-            phase[t] = (np >= a.pat_period[t]) ? np - a.pat_period[t] : np;
-          }
-        }
-        if (c == 0 && segLow <= a.presieve_max) {
-          // The patterns also cleared the pre-sieve primes themselves;
-          // put them back (reference: restore bytes, GpuTables.cpp:108-127).
-          uint32_t w4[4] = { v.x, v.y, v.z, v.w };
-          for (uint32_t i = 0; i < a.num_presieve_primes; i++) {
-            const uint64_t q = a.presieve_primes[i];
-            if (q < segLow + 7) continue;
-            const uint64_t rel = q - segLow - 7;      // < 16*30
-            const uint32_t byte = (uint32_t) (rel / 30u);
-            if (byte >= 16) continue;
-            const uint32_t bit = residue_to_bit((uint32_t) (q % 30u));
-            w4[byte >> 2] |= 1u << (8 * (byte & 3) + bit);
-          }
-          v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-        }
-        smem4[c] = v;
-      }
-    }
+    phase_presieve<BLOCK>(a, smem4, segLow, tid);
     __syncthreads();
-
-    // ---- 2. small primes: one warp per prime ----------------------------
-    {
-      const uint32_t j = lane & 7u;
-      const uint32_t r = lane >> 3;
-      const uint32_t Q = cofactor_class(j);
-      const uint64_t x0 = segLow + 7;
-#pragma unroll
-      for (int m = 0; m < SREG; m++) {
-        const uint32_t tbase = 32u * m;
-        if (warp + NWARPS * tbase >= a.n_small) break;
-        for (uint32_t l = 0; l < 32; l++) {
-          const uint32_t idx = warp + NWARPS * (tbase + l);
-          if (idx >= a.n_small) break;
-          const uint32_t p = __shfl_sync(0xffffffffu, sp[m], l);
-          const uint32_t rem = __shfl_sync(0xffffffffu, sr[m], l);
-          const uint32_t pm = p % 30u;
-          const uint64_t pp = (uint64_t) p * p;
-          uint64_t d; uint32_t c0;
-          if (x0 <= pp) {
-            d = pp - x0;
-            c0 = pm;
-            if (d >= span) continue;
-          } else {
-            const uint32_t dd = rem ? p - rem : 0u;
-            d = dd;
-            c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
-          }
-          const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
-          const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
-          if (b64 < seg_bytes) {
-            const uint32_t b = (uint32_t) b64;
-            const uint32_t bit = residue_to_bit((Q * pm) % 30u);
-            const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
-            for (uint32_t w = b >> 2; w < nwords; w += p)
-              atomicAnd(&sieve32[w], mask);
-          }
-        }
-      }
-      // small primes beyond the register-resident ones
-      for (uint32_t idx = warp + NWARPS * 32u * SREG; idx < a.n_small; idx += NWARPS) {
-        const uint32_t p = a.primes[idx];
-        uint64_t d; uint32_t c0;
-        first_multiple(segLow, p, a.recip[idx], d, c0);
-        if (d >= span) continue;
-        const uint32_t pm = p % 30u;
-        const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
-        const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
-        if (b64 < seg_bytes) {
-          const uint32_t b = (uint32_t) b64;
-          const uint32_t bit = residue_to_bit((Q * pm) % 30u);
-          const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
-          for (uint32_t w = b >> 2; w < nwords; w += p)
-            atomicAnd(&sieve32[w], mask);
-        }
-      }
-    }
-
-    // ---- 3. medium primes: one thread per prime, carried wheel walk ------
-    {
-      uint32_t i = tid;
-      uint32_t p = 0;
-      if (i < n_med) p = a.primes[a.n_small + i];
-      for (; i < n_med; i += BLOCK) {
-        const uint32_t inext = i + BLOCK;
-        const uint32_t pn = (inext < n_med) ? a.primes[a.n_small + inext] : 0u;
-        uint32_t st = mstate[i];
-        if (st == kFar) {
-          uint64_t d; uint32_t c0;
-          first_multiple(segLow, p, a.recip[a.n_small + i], d, c0);
-          const uint32_t j0 = first_class_ge(c0);
-          const uint64_t b = (d + (uint64_t) (cofactor_class(j0) - c0) * p) / 30u;
-          st = (b < (1ull << 29) - 1) ? (uint32_t) (b << 3) | j0 : kFar;
-        }
-        if (st != kFar) {
-          uint32_t b = st >> 3;
-          uint32_t j = st & 7u;
-          if (b < seg_bytes) {
-            const uint32_t pdiv30 = p / 30u;
-            const uint32_t cls = residue_to_bit(p - 30u * pdiv30);
-            const uint32_t bits = wheel_tab[2 * cls];
-            const uint32_t corr = wheel_tab[2 * cls + 1];
-            do {
-              const uint32_t sh = 3u * j;
-              const uint32_t bit = (bits >> sh) & 7u;
-              atomicAnd(&sieve32[b >> 2], ~(1u << (bit + 8u * (b & 3u))));
-              b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
-              j = (j + 1u) & 7u;
-            } while (b < seg_bytes);
-          }
-          const uint32_t nb = b - seg_bytes;
-          st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kFar;
-        }
-        mstate[i] = st;
-        p = pn;
-      }
-    }
-
-    // ---- 4. big primes: bucket lists of this segment ---------------------
-    // Warps take lists from a shared counter (lists differ in length); each
-    // lane applies 4 entries per 16-byte load (lists start 16-byte aligned).
-    if (a.num_bucket_lists) {
-      const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
-      const uint32_t* seg_entries = a.bucket_entries + s * a.bucket_seg_stride;
-      for (;;) {
-        uint32_t l = 0;
-        if (lane == 0) l = atomicAdd(&list_next, 1u);
-        l = __shfl_sync(0xffffffffu, l, 0);
-        if (l >= a.num_bucket_lists) break;
-        const uint32_t n = cnt[l];
-        const uint32_t* e = seg_entries + a.bucket_list_off[l];
-        const uint32_t n4 = n & ~3u;
-        for (uint32_t x = 4 * lane; x < n4; x += 128) {
-          const uint4 v4 = __ldg(reinterpret_cast<const uint4*>(e + x));
-          const uint32_t v[4] = { v4.x, v4.y, v4.z, v4.w };
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const uint32_t bb = v[q] >> 3;       // entry: byte index << 3 | bit
-            atomicAnd(&sieve32[bb >> 2], ~(1u << ((v[q] & 7u) + 8u * (bb & 3u))));
-          }
-        }
-        if (n4 + lane < n) {
-          const uint32_t v = __ldg(e + n4 + lane);
-          const uint32_t bb = v >> 3;
-          atomicAnd(&sieve32[bb >> 2], ~(1u << ((v & 7u) + 8u * (bb & 3u))));
-        }
-      }
-    }
+    phase_small<BLOCK>(a, a.n_small, sieve32, segLow, warp, lane, sp, sr);
+    phase_medium<BLOCK>(a, a.n_small, n_med, mstate, sieve32, wheel_tab, segLow, tid);
+    phase_direct<BLOCK>(a, a.n_primes, a.n_direct, sieve32, wheel_tab, segLow, tid);
+    if (a.num_bucket_lists) phase_buckets(a, s, sieve32, &list_next, lane);
     __syncthreads();
-
-    // ---- 5. mask the range edges and count -------------------------------
-    {
-      const uint64_t rhi = a.hi - segLow;                   // >= 7
-      const uint64_t rlo = (a.lo > segLow) ? a.lo - segLow : 0;
-      const bool full = (rlo <= 7) && (rhi >= span + 1);
-      uint32_t c[6] = { 0, 0, 0, 0, 0, 0 };
-      for (uint32_t ch = tid; ch < nchunks; ch += BLOCK) {
-        uint4 v = smem4[ch];
-        if (!full) {
-          uint32_t w4[4] = { v.x, v.y, v.z, v.w };
-#pragma unroll
-          for (int q = 0; q < 4; q++) {
-            uint32_t m = 0;
-#pragma unroll
-            for (int by = 0; by < 4; by++) {
-              const uint64_t base = 30ull * (16ull * ch + 4u * q + by);
-              m |= byte_keep(base, rlo, rhi) << (8 * by);
-            }
-            w4[q] &= m;
-          }
-          v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-        }
-        count_word<ALL_KINDS>(v.x, c);
-        count_word<ALL_KINDS>(v.y, c);
-        count_word<ALL_KINDS>(v.z, c);
-        count_word<ALL_KINDS>(v.w, c);
-      }
-#pragma unroll
-      for (int k = 0; k < 6; k++) acc[k] += c[k];
-    }
-
-    // advance the small primes' remainders to the next segment
-#pragma unroll
-    for (int m = 0; m < SREG; m++) {
-      const uint32_t nr = sr[m] + sdl[m];
-      sr[m] = (nr >= sp[m]) ? nr - sp[m] : nr;
-    }
+    phase_count<BLOCK, ALL_KINDS>(smem4, a.seg_bytes, segLow, a.lo, a.hi, tid, acc);
+    small_advance(sp, sr, sdl);
     __syncthreads();
   }
-
-  // ---- warp reduction, one atomic per warp and kind ----------------------
-#pragma unroll
-  for (int k = 0; k < 6; k++) {
-    if (!ALL_KINDS && k > 0) break;
-    uint64_t v = acc[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0 && v && ((a.kinds >> k) & 1u))
-      atomicAdd(&a.counts[k], (unsigned long long) v);
-  }
+  flush_counts<ALL_KINDS>(acc, a.kinds, a.counts, lane);
 }
 
 } // namespace psg

@@ -82,3 +82,23 @@ def test_empty_and_tiny(oracle):
     assert oracle.plain(0, 17) == [7, 3, 3, 1, 1, 0]      # incl. (5,7,11,13,17)
     top = 2 ** 64 - 1
     assert oracle.plain(top, top) == [0] * 6               # 2^64-1 is composite
+
+
+def test_batch_fixture_pinned(oracle):
+    """The 4096-range fixture: its ranges regenerate from the documented RNG
+    recipe, and its shortest rows (counts from the reference library) agree
+    with the oracle."""
+    import importlib.util
+    import json
+    import os
+    from conftest import REPO
+    golden = os.path.join(REPO, "tests", "golden")
+    spec = importlib.util.spec_from_file_location("make_batch", os.path.join(golden, "make_batch.py"))
+    mb = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mb)
+    with open(os.path.join(golden, "batch4096.json")) as f:
+        rows = json.load(f)["ranges"]
+    assert [tuple(r[:3]) for r in rows] == mb.make_ranges(4096, 0)
+    short = sorted(rows, key=lambda r: r[1] - r[0])[:40]
+    for a, b, k, want in short:
+        assert oracle.plain(a, b, 1 << k)[k] == want, (a, b, k)
