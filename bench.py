@@ -184,6 +184,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-per-range section")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -304,6 +305,10 @@ def main():
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
                "sample": f"[1e15, 1e15+{n:.3g}] in {el:.1f} s, -t {cores}"}
 
+    batched = None
+    if not args.no_batch:
+        batched = batch_section(psg, ctx, rank, world, args, torch, dist)
+
     if rank == 0:
         cfg = ctx.config()
         line = {
@@ -322,6 +327,7 @@ def main():
                     "api": "psg_count (C ABI, host result)"},
             "gpu_launches": launches,
             "clocks": clk,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -329,6 +335,109 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return 0 if ok0 else 1
+
+
+BATCH_FIXTURE = os.path.join(REPO, "tests", "golden", "batch4096.json")
+BATCH_WORKLOAD = ("4096 ranges, seed 0: start log-uniform [1e6, 1e16], length log-uniform "
+                  "[2^16, 2^34], kind uniform over primes/twins/triplets")
+
+
+def batch_section(psg, ctx, rank, world, args, torch, dist):
+    """Batched vs per-range on the 4096-range workload (rank r takes ranges
+    i = r mod N). Both arms go through the C ABI with host arguments and host
+    results: per-range = one psg_count() per range, batched = one
+    psg_count_batch() for all of them. Wall clock, max over ranks."""
+    with open(BATCH_FIXTURE) as f:
+        rows = json.load(f)["ranges"]
+    mine = [r for i, r in enumerate(rows) if i % world == rank]
+    q = [(a, b, 1 << k) for a, b, k, _ in mine]
+    ints = sum(b - a + 1 for a, b, _, _ in rows)
+    ctx.prepare(max(b for _, b, _, _ in rows))
+
+    def check(res):
+        return all(r[k] == want and not any(r[j] for j in range(6) if j != k)
+                   for (a, b, k, want), r in zip(mine, res))
+
+    def tmax(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx.count_batch(q[:64])                      # warm-up
+    ok = True
+    times = []
+    for _ in range(2):
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        res = ctx.count_batch(q)
+        times.append(tmax(time.perf_counter() - t))
+        ok = ok and check(res)
+    ctx.set_profiling(True)
+    ctx.reset_kernel_stats()
+    ctx.count_batch(q)
+    kst = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    if world > 1:
+        dist.barrier()
+    t = time.perf_counter()
+    res = [ctx.count(a, b, k) for a, b, k in q]
+    t_single = tmax(time.perf_counter() - t)
+    ok = ok and check(res)
+    ok_t = torch.tensor([1 if ok else 0], dtype=torch.int64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ok_t, op=dist.ReduceOp.MIN)
+    t_batch = min(times)
+    out = {
+        "workload": BATCH_WORKLOAD, "ranges": len(rows), "integers": ints,
+        "value": ints / t_batch, "unit": UNIT, "seconds": t_batch,
+        "per_range_value": ints / t_single, "per_range_seconds": t_single,
+        "speedup_vs_per_range": t_single / t_batch,
+        "count_ok": bool(ok_t.item()),
+        "kernel_ms": {k: round(v[1], 2) for k, v in kst.items() if v[0]},
+        "kernel_launches": {k: v[0] for k, v in kst.items() if v[0]},
+        "api": "psg_count_batch vs psg_count per range (C ABI, host results)",
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_batch_rate(rows, 10.0)
+        out["vs_cpu"] = out["value"] / out["cpu_baseline"]["value"]
+    return out
+
+
+def cpu_batch_rate(rows, budget_s):
+    """The reference library (oracle/_ref/libprimesieve_ref.so) counting a
+    seeded random sample of the batch ranges one call at a time with all
+    host threads, as the reference's callers would; stops after budget_s."""
+    import ctypes
+    import random
+    lib_path = os.path.join(REPO, "oracle", "_ref", "libprimesieve_ref.so")
+    if not os.path.exists(lib_path):
+        return None
+    lib = ctypes.CDLL(lib_path)
+    cores = os.cpu_count() or 1
+    lib.primesieve_set_num_threads.argtypes = [ctypes.c_int]
+    lib.primesieve_set_num_threads(cores)
+    fns = []
+    for name in ("primes", "twins", "triplets"):
+        f = getattr(lib, "primesieve_count_" + name)
+        f.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        f.restype = ctypes.c_uint64
+        fns.append(f)
+    order = list(range(len(rows)))
+    random.Random(0).shuffle(order)
+    done, ints, t0 = 0, 0, time.perf_counter()
+    for i in order:
+        a, b, k, want = rows[i]
+        if fns[k](a, b) != want:
+            raise RuntimeError("reference library disagrees with the fixture")
+        done += 1
+        ints += b - a + 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": ints / el, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{done} of {len(rows)} ranges (seeded shuffle), {ints:.3g} integers in {el:.1f} s"}
 
 
 def crossing_count(stop):

@@ -150,6 +150,50 @@ int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s);
 int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
                       uint64_t* dev_counts, void* stream);
 
+/* ---- request server: continuous batching -------------------------------
+ * No reference counterpart (the reference answers one count per call,
+ * src/api.cpp:48-118). A worker thread owns the context's GPU and runs it in
+ * steps: each step admits waiting requests into free device slots, runs one
+ * launch of the persistent batch kernel over segment stripes taken
+ * round-robin from the admitted requests plus one bucket window of the
+ * oldest long high request, and completes the requests whose last piece ran.
+ * Requests that arrive meanwhile join the next step. The sieving-prime table
+ * stays resident (up to prime_limit, 2^32 by default: every 64-bit stop).
+ * A request whose bucket storage would exceed the HBM budget is refused
+ * with PSG_ERR_NOMEM. The context must outlive the server; other calls on
+ * the context wait for the current step. */
+typedef struct psg_server psg_server;
+
+typedef struct {
+  uint32_t max_slots;          /* requests on the device at once; 0 = 4096 */
+  uint32_t step_segments;      /* batch-kernel segments per step; 0 = auto */
+  uint64_t prime_limit;        /* resident sieving primes up to; 0 = 2^32 - 1 */
+  uint64_t hbm_budget;         /* bytes of bucket storage allowed; 0 = 80% of free HBM */
+} psg_server_config;
+
+typedef struct {
+  uint64_t submitted, completed, refused, steps;
+  uint64_t bucket_requests;    /* admitted on the windowed bucket path */
+  uint64_t batch_requests;     /* admitted on the persistent batch kernel */
+  double integers;             /* integers of completed requests */
+  double gpu_busy_seconds;     /* wall time spent in steps */
+} psg_server_stats;
+
+int psg_server_start(psg_context* ctx, const psg_server_config* cfg, psg_server** out);
+/* Queue a count of [start, stop] (kinds mask); *id names it for wait. */
+int psg_server_submit(psg_server* s, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t* id);
+/* Block until request id is done: counts[6] and its latency (seconds from
+ * submit to completion). Returns the request's status. */
+int psg_server_wait(psg_server* s, uint64_t id, uint64_t counts[6], double* latency_seconds);
+/* Load replay: submits requests[i] at arrival_seconds[i] after the call
+ * (ascending), waits for all; counts is n x 6, latency from the scheduled
+ * arrival. */
+int psg_server_replay(psg_server* s, const psg_range* requests, const double* arrival_seconds,
+                      size_t n, uint64_t* counts, double* latency_seconds);
+int psg_server_get_stats(psg_server* s, psg_server_stats* out);
+/* Stops the worker (requests still queued fail with PSG_ERR_CLOSED). */
+void psg_server_stop(psg_server* s);
+
 /* The library version string. */
 const char* psg_version(void);
 

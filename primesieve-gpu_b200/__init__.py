@@ -28,6 +28,8 @@ PSG_SYMBOLS = (
     "psg_count_batch", "psg_prepare", "psg_last_error", "psg_status_string",
     "psg_set_profiling", "psg_kernel_stats", "psg_reset_kernel_stats", "psg_version",
     "psg_bucket_entries", "psg_measure_smem_atomic_rate", "psg_count_noalloc",
+    "psg_server_start", "psg_server_submit", "psg_server_wait", "psg_server_replay",
+    "psg_server_get_stats", "psg_server_stop",
 )
 
 
@@ -48,6 +50,18 @@ class PsgConfig(ctypes.Structure):
 class PsgRange(ctypes.Structure):
     _fields_ = [("start", ctypes.c_uint64), ("stop", ctypes.c_uint64),
                 ("kinds", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class PsgServerConfig(ctypes.Structure):
+    _fields_ = [("max_slots", ctypes.c_uint32), ("step_segments", ctypes.c_uint32),
+                ("prime_limit", ctypes.c_uint64), ("hbm_budget", ctypes.c_uint64)]
+
+
+class PsgServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("refused", ctypes.c_uint64), ("steps", ctypes.c_uint64),
+                ("bucket_requests", ctypes.c_uint64), ("batch_requests", ctypes.c_uint64),
+                ("integers", ctypes.c_double), ("gpu_busy_seconds", ctypes.c_double)]
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -86,6 +100,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_measure_smem_atomic_rate.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     lib.psg_count_noalloc.argtypes = [u64, u64, u32, vp, vp]
     lib.psg_version.restype = ctypes.c_char_p
+    DP = ctypes.POINTER(ctypes.c_double)
+    lib.psg_server_start.argtypes = [vp, ctypes.POINTER(PsgServerConfig), ctypes.POINTER(vp)]
+    lib.psg_server_submit.argtypes = [vp, u64, u64, u32, U64P]
+    lib.psg_server_wait.argtypes = [vp, u64, U64P, DP]
+    lib.psg_server_replay.argtypes = [vp, ctypes.POINTER(PsgRange), DP, sz, U64P, DP]
+    lib.psg_server_get_stats.argtypes = [vp, ctypes.POINTER(PsgServerStats)]
+    lib.psg_server_stop.argtypes = [vp]
+    lib.psg_server_stop.restype = None
     for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
         fn = getattr(lib, "primesieve_count_" + name, None)
         if fn is not None:
@@ -198,6 +220,84 @@ class Context:
         v = ctypes.c_uint64(0)
         _check(self._lib.psg_bucket_entries(self._h, ctypes.byref(v), 1 if reset else 0))
         return v.value
+
+
+class Server:
+    """Request server with continuous batching on a context (psg_server_*).
+    The context must stay open while the server runs."""
+
+    def __init__(self, ctx: "Context", **config: int):
+        lib = load()
+        cfg = PsgServerConfig()
+        for k, v in config.items():
+            setattr(cfg, k, int(v))
+        h = ctypes.c_void_p()
+        _check(lib.psg_server_start(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    def submit(self, start: int, stop: int, kinds: int = 0x3F) -> int:
+        rid = ctypes.c_uint64(0)
+        _check(self._lib.psg_server_submit(self._h, start, stop, kinds, ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid: int) -> Tuple[List[int], float]:
+        out = (ctypes.c_uint64 * 6)()
+        lat = ctypes.c_double(0)
+        _check(self._lib.psg_server_wait(self._h, rid, out, ctypes.byref(lat)))
+        return list(out), lat.value
+
+    def replay(self, requests: Sequence[Tuple[int, int, int]], arrivals: Sequence[float]):
+        """Submit requests[i] at arrivals[i] seconds; returns (counts, latencies)."""
+        n = len(requests)
+        arr = (PsgRange * max(n, 1))()
+        for i, (a, b, k) in enumerate(requests):
+            arr[i].start, arr[i].stop, arr[i].kinds = a, b, k
+        t = (ctypes.c_double * max(n, 1))(*arrivals)
+        out = (ctypes.c_uint64 * (6 * max(n, 1)))()
+        lat = (ctypes.c_double * max(n, 1))()
+        _check(self._lib.psg_server_replay(self._h, arr, t, n, out, lat))
+        return [list(out[6 * i:6 * i + 6]) for i in range(n)], list(lat[:n])
+
+    def stats(self) -> dict:
+        st = PsgServerStats()
+        _check(self._lib.psg_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in PsgServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.psg_server_stop(self._h)
+            self._h = None
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+
+def serving_workload(n: int, rate: float, seed: int = 1, len_log2: Tuple[float, float] = (12.0, 36.0),
+                     start_range: Tuple[float, float] = (1e6, 1.8e19)):
+    """The serving request stream: Poisson arrivals at `rate` requests/s,
+    start log-uniform in start_range, length log-uniform in 2^len_log2,
+    kind uniform over 1..6 (primes .. sextuplets), stop clamped to 2^64 - 1.
+    numpy.random.default_rng(seed), drawn per request in the order
+    gap, start, length, kind. Returns (requests [(start, stop, kinds)],
+    arrival seconds)."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log10(start_range[0]), math.log10(start_range[1])
+    reqs, arrivals, t = [], [], 0.0
+    for _ in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        start = int(10.0 ** rng.uniform(lo, hi))
+        length = int(2.0 ** rng.uniform(len_log2[0], len_log2[1]))
+        kind = int(rng.integers(1, 7))
+        stop = min(start + length - 1, (1 << 64) - 1)
+        reqs.append((start, stop, 1 << (kind - 1)))
+        arrivals.append(t)
+    return reqs, arrivals
 
 
 def split_range(start: int, stop: int, parts: int) -> List[Tuple[int, int]]:

@@ -54,13 +54,92 @@ int grow(T*& ptr, size_t& cap, size_t n, std::string& err) {
 
 } // namespace
 
+uint64_t Engine::range_segments(const BatchRange& r) const {
+  return (r.hi - 7 - r.seg_low0) / ((uint64_t) seg_bytes_ * 30u) + 1;
+}
+
+// Batch-kernel tiers of [lo, hi] (lo >= 7); false when the range has so many
+// primes beyond the shared state for its length that the bucket path is
+// cheaper. seg_cost: relative cost of one of its segments.
+bool Engine::batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r, double& seg_cost) {
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  const uint32_t n_small_all = count_primes_le(small_limit_, true);   // inside the exact head
+  const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
+  const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
+  const uint32_t n_total = count_primes_upper(isqrt_u64(hi));
+  const uint32_t n_small = std::min(n_small_all, n_total);
+  const uint32_t n_med = std::max(n_small, std::min(n_total, n_small_all + state_cap_));
+  const double direct = (double) (n_total - n_med);
+  if (direct > 0 && (direct * (double) nseg > kDirectBudget || nseg >= (1ull << 32))) return false;
+  r.seg_low0 = seg_low0;
+  r.lo = lo;
+  r.hi = hi;
+  r.n_small = n_small;
+  r.n_med_end = n_med;
+  r.n_end = n_total;
+  r.kinds = kinds;
+  // sieve work + one reciprocal per direct prime
+  seg_cost = 1.0 + direct / 2.0e4;
+  return true;
+}
+
+// Stripes of <= kStripe segments of range `k` from segment s0 on, at most
+// max_seg segments in all; returns the segment after the last one taken.
+uint64_t Engine::append_stripes(uint32_t k, const BatchRange& r, double seg_cost, uint64_t s0, uint64_t max_seg,
+                                std::vector<BatchItem>& items, std::vector<double>& cost) const {
+  const uint64_t nseg = range_segments(r);
+  const uint64_t nst = (nseg + kStripe - 1) / kStripe;
+  const uint64_t len = (nseg + nst - 1) / nst;
+  uint64_t taken = 0;
+  while (s0 < nseg && taken < max_seg) {
+    BatchItem it;
+    it.range = k;
+    it.seg0 = (uint32_t) s0;
+    it.nseg = (uint32_t) std::min<uint64_t>(len, nseg - s0);
+    it.pad = 0;
+    items.push_back(it);
+    cost.push_back(seg_cost * it.nseg);
+    s0 += it.nseg;
+    taken += it.nseg;
+  }
+  return s0;
+}
+
+void Engine::sort_items(std::vector<BatchItem>& items, const std::vector<double>& cost) {
+  std::vector<uint32_t> order(items.size());
+  for (size_t i = 0; i < order.size(); i++) order[i] = (uint32_t) i;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return cost[x] > cost[y]; });
+  std::vector<BatchItem> sorted(items.size());
+  for (size_t i = 0; i < order.size(); i++) sorted[i] = items[order[i]];
+  items.swap(sorted);
+}
+
+// The persistent batch kernel over n_items device items (queue zeroed here).
+int Engine::launch_items(const BatchRange* d_ranges, const BatchItem* d_items, uint32_t n_items,
+                         unsigned long long* d_rows, uint32_t* d_queue, cudaStream_t st, std::string& err) {
+  if (n_items == 0) return PSG_OK;
+  PSG_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(uint32_t), st));
+  BatchArgs b;
+  std::memset(&b, 0, sizeof b);
+  fill_common_args(b.common);
+  b.ranges = d_ranges;
+  b.items = d_items;
+  b.num_items = n_items;
+  b.queue = d_queue;
+  b.counts = d_rows;
+  timed_begin(3, st);
+  cudaError_t e = launch_batch(b, st);
+  timed_end(3, st);
+  if (e != cudaSuccess) { err = std::string("batch kernel launch: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+  return PSG_OK;
+}
+
 int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::string& err) {
   PSG_CUDA(cudaSetDevice(device_));
   std::fill(out, out + 6 * n, 0ull);
   // the engine's scratch is shared with counts queued on other streams
   if (last_stream_ && last_stream_ != stream_) PSG_CUDA(cudaStreamWaitEvent(stream_, done_event_, 0));
   if (n == 0) return PSG_OK;
-  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
 
   // ---- 1. host part of every range, largest stop
   std::vector<uint64_t> lo(n, 0), hi(n, 0);
@@ -83,62 +162,29 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   if (rc) return rc;
 
   // ---- 2. tiers and class of every range
-  const uint32_t n_small_all = count_primes_le(small_limit_, true);
   std::vector<BatchRange> br;
   std::vector<size_t> br_index;             // batch range -> query
   std::vector<size_t> bucket_ranges;        // queries for the windowed path
   std::vector<double> seg_cost;             // per batch range: cost of one segment
   for (size_t i = 0; i < n; i++) {
     if (!kinds[i]) continue;
-    const uint64_t seg_low0 = lo[i] - ((lo[i] - 7) % 30 + 7);
-    const uint64_t nseg = (hi[i] - 7 - seg_low0) / span + 1;
-    const uint32_t n_total = count_primes_upper(isqrt_u64(hi[i]));
-    const uint32_t n_small = std::min(n_small_all, n_total);
-    const uint32_t n_med = std::max(n_small, std::min(n_total, n_small_all + state_cap_));
-    const double direct = (double) (n_total - n_med);
-    if (direct > 0 && (direct * (double) nseg > kDirectBudget || nseg >= (1ull << 32))) {
+    BatchRange r;
+    double c = 0;
+    if (!batch_range(lo[i], hi[i], kinds[i], r, c)) {
       bucket_ranges.push_back(i);
       continue;
     }
-    BatchRange r;
-    r.seg_low0 = seg_low0;
-    r.lo = lo[i];
-    r.hi = hi[i];
-    r.n_small = n_small;
-    r.n_med_end = n_med;
-    r.n_end = n_total;
-    r.kinds = kinds[i];
     br.push_back(r);
     br_index.push_back(i);
-    // relative cost of one segment: sieve work + one reciprocal per direct prime
-    seg_cost.push_back(1.0 + direct / 2.0e4);
+    seg_cost.push_back(c);
   }
 
   // ---- 3. work items: stripes of <= kStripe segments, most expensive first
   std::vector<BatchItem> items;
   std::vector<double> item_cost;
-  for (size_t k = 0; k < br.size(); k++) {
-    const uint64_t nseg = (br[k].hi - 7 - br[k].seg_low0) / span + 1;
-    const uint64_t nst = (nseg + kStripe - 1) / kStripe;
-    const uint64_t len = (nseg + nst - 1) / nst;
-    for (uint64_t s0 = 0; s0 < nseg; s0 += len) {
-      BatchItem it;
-      it.range = (uint32_t) k;
-      it.seg0 = (uint32_t) s0;
-      it.nseg = (uint32_t) std::min<uint64_t>(len, nseg - s0);
-      it.pad = 0;
-      items.push_back(it);
-      item_cost.push_back(seg_cost[k] * it.nseg);
-    }
-  }
-  {
-    std::vector<uint32_t> order(items.size());
-    for (size_t i = 0; i < order.size(); i++) order[i] = (uint32_t) i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return item_cost[x] > item_cost[y]; });
-    std::vector<BatchItem> sorted(items.size());
-    for (size_t i = 0; i < order.size(); i++) sorted[i] = items[order[i]];
-    items.swap(sorted);
-  }
+  for (size_t k = 0; k < br.size(); k++)
+    append_stripes((uint32_t) k, br[k], seg_cost[k], 0, ~0ull, items, item_cost);
+  sort_items(items, item_cost);
   batch_direct_ranges_ = br.size();
   batch_bucket_ranges_ = bucket_ranges.size();
   batch_items_ = items.size();
@@ -155,19 +201,9 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   if (!items.empty()) {
     PSG_CUDA(cudaMemcpyAsync(d_batch_ranges_, br.data(), br.size() * sizeof(BatchRange), cudaMemcpyHostToDevice, stream_));
     PSG_CUDA(cudaMemcpyAsync(d_batch_items_, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, stream_));
-    PSG_CUDA(cudaMemsetAsync(d_batch_queue_, 0, sizeof(uint32_t), stream_));
-    BatchArgs b;
-    std::memset(&b, 0, sizeof b);
-    fill_common_args(b.common);
-    b.ranges = d_batch_ranges_;
-    b.items = d_batch_items_;
-    b.num_items = (uint32_t) items.size();
-    b.queue = d_batch_queue_;
-    b.counts = d_batch_rows_;
-    timed_begin(3, stream_);
-    cudaError_t e = launch_batch(b);
-    timed_end(3, stream_);
-    if (e != cudaSuccess) { err = std::string("batch kernel launch: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+    rc = launch_items(d_batch_ranges_, d_batch_items_, (uint32_t) items.size(), d_batch_rows_,
+                      d_batch_queue_, stream_, err);
+    if (rc) return rc;
   }
   for (size_t j = 0; j < bucket_ranges.size(); j++) {
     const size_t i = bucket_ranges[j];
@@ -201,20 +237,20 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   return PSG_OK;
 }
 
-cudaError_t Engine::launch_batch(const BatchArgs& b) {
+cudaError_t Engine::launch_batch(const BatchArgs& b, cudaStream_t st) {
   static_assert(sizeof(BatchArgs) < 4000, "kernel parameter space");
   switch (block_) {
     case 256:
       cudaFuncSetAttribute(batch_sieve_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
-      batch_sieve_kernel<256><<<grid_, 256, smem_dyn_, stream_>>>(b);
+      batch_sieve_kernel<256><<<grid_, 256, smem_dyn_, st>>>(b);
       break;
     case 1024:
       cudaFuncSetAttribute(batch_sieve_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
-      batch_sieve_kernel<1024><<<grid_, 1024, smem_dyn_, stream_>>>(b);
+      batch_sieve_kernel<1024><<<grid_, 1024, smem_dyn_, st>>>(b);
       break;
     default:
       cudaFuncSetAttribute(batch_sieve_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dyn_);
-      batch_sieve_kernel<512><<<grid_, 512, smem_dyn_, stream_>>>(b);
+      batch_sieve_kernel<512><<<grid_, 512, smem_dyn_, st>>>(b);
       break;
   }
   return cudaGetLastError();

@@ -14,24 +14,9 @@
 #include <stdint.h>
 #include <cuda_runtime.h>
 #include "sieve_kernel.cuh"
+#include "batch_types.hpp"
 
 namespace psg {
-
-struct BatchRange {
-  uint64_t seg_low0;            // multiple of 30
-  uint64_t lo, hi;              // inclusive, 7 <= lo <= hi
-  uint32_t n_small;             // primes[0, n_small): warp per prime
-  uint32_t n_med_end;           // primes[n_small, n_med_end): carried state
-  uint32_t n_end;               // primes[n_med_end, n_end): direct
-  uint32_t kinds;
-};
-
-struct BatchItem {
-  uint32_t range;
-  uint32_t seg0;                // first segment of the stripe
-  uint32_t nseg;                // >= 1
-  uint32_t pad;
-};
 
 struct BatchArgs {
   SieveArgs common;             // tables, primes, segment size (range fields unused)

@@ -5,6 +5,7 @@
 // serialises every GPU call with one global mutex, src/gpu/GpuSieve.cpp:27).
 #include "../../include/psgpu.h"
 #include "engine.hpp"
+#include "server.hpp"
 
 #include <cuda_runtime.h>
 #include <cstdio>
@@ -18,6 +19,10 @@
 struct psg_context {
   psg::Engine engine;
   std::mutex mu;
+};
+
+struct psg_server {
+  std::unique_ptr<psg::Server> srv;
 };
 
 namespace {
@@ -53,6 +58,70 @@ void set_last_error(const std::string& msg) { t_last_error = msg; }
 }
 
 extern "C" {
+
+int psg_server_start(psg_context* ctx, const psg_server_config* cfg, psg_server** out) {
+  if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
+  *out = nullptr;
+  psg::ServerConfig c;
+  if (cfg) {
+    c.max_slots = cfg->max_slots;
+    c.step_segments = cfg->step_segments;
+    c.prime_limit = cfg->prime_limit;
+    c.hbm_budget = cfg->hbm_budget;
+  }
+  std::unique_ptr<psg_server> s(new (std::nothrow) psg_server{ std::make_unique<psg::Server>(ctx->engine, ctx->mu) });
+  if (!s) return fail(PSG_ERR_NOMEM, "out of host memory");
+  std::string err;
+  int rc = s->srv->start(c, err);
+  if (rc) return fail(rc, err);
+  *out = s.release();
+  return PSG_OK;
+}
+
+int psg_server_submit(psg_server* s, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t* id) {
+  if (!s || !id) return fail(PSG_ERR_ARG, "NULL argument");
+  std::string err;
+  int rc = s->srv->submit(start, stop, kinds, *id, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_server_wait(psg_server* s, uint64_t id, uint64_t counts[6], double* latency_seconds) {
+  if (!s) return fail(PSG_ERR_ARG, "NULL argument");
+  std::string err;
+  int rc = s->srv->wait(id, counts, latency_seconds, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_server_replay(psg_server* s, const psg_range* requests, const double* arrival_seconds,
+                      size_t n, uint64_t* counts, double* latency_seconds) {
+  if (!s || (n && (!requests || !arrival_seconds))) return fail(PSG_ERR_ARG, "NULL argument");
+  for (size_t i = 1; i < n; i++)
+    if (arrival_seconds[i] < arrival_seconds[i - 1]) return fail(PSG_ERR_ARG, "arrival times must ascend");
+  std::string err;
+  int rc = s->srv->replay(reinterpret_cast<const psg::RangeQuery*>(requests), arrival_seconds, n, counts,
+                          latency_seconds, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_server_get_stats(psg_server* s, psg_server_stats* out) {
+  if (!s || !out) return fail(PSG_ERR_ARG, "NULL argument");
+  const psg::ServerStats st = s->srv->stats();
+  out->submitted = st.submitted;
+  out->completed = st.completed;
+  out->refused = st.refused;
+  out->steps = st.steps;
+  out->bucket_requests = st.bucket_requests;
+  out->batch_requests = st.batch_requests;
+  out->integers = st.integers;
+  out->gpu_busy_seconds = st.gpu_busy_seconds;
+  return PSG_OK;
+}
+
+void psg_server_stop(psg_server* s) {
+  if (!s) return;
+  s->srv->stop();
+  delete s;
+}
 
 const char* psg_version(void) { return "primesieve-b200 1.0 (primesieve 12.16 count API)"; }
 

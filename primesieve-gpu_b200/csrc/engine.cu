@@ -716,6 +716,18 @@ void Engine::reset_kernel_stats() {
   for (auto& t : timed_) { t.launches = 0; t.ms = 0; }
 }
 
+// Bucket storage the windows of p need: per segment, every list's expected
+// entries plus its margin (as ensure_buckets sizes them), times the window.
+size_t Engine::bucket_bytes(const RangePlan& p) const {
+  if (!p.buckets) return 0;
+  const double per_seg = (double) seg_bytes_ * 30.0 * (8.0 / 30.0);
+  const double total = per_seg * (inv_prefix(p.n_total) - inv_prefix(p.n_dir));
+  const double lists = std::max<double>(1.0, std::min<double>(lists_, p.n_total - p.n_dir));
+  const double mu = total / lists;
+  const double stride = lists * (mu + 6.0 * std::sqrt(mu) + 36.0) * cap_scale_;
+  return (size_t) (stride * (double) window_ * 4.0);
+}
+
 // Launch-wide sieve arguments: segment size, pre-sieve tables, sieving
 // primes and the wheel walk tables (range and tier fields zero).
 void Engine::fill_common_args(SieveArgs& a) const {
@@ -740,46 +752,68 @@ void Engine::fill_common_args(SieveArgs& a) const {
   }
 }
 
-int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
-                cudaStream_t st, std::string& err) {
-  // lo >= 7, lo <= hi
+// Prime tiers and launch geometry of [lo, hi] (lo >= 7, lo <= hi).
+int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err) {
   const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  p.lo = lo;
+  p.hi = hi;
   // byteRemainder (reference src/Erat.cpp:231-237, CudaBackend.cpp:457)
-  const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
-  const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
+  p.seg_low0 = lo - ((lo - 7) % 30 + 7);
+  p.nseg = (hi - 7 - p.seg_low0) / span + 1;
   const uint32_t sq = isqrt_u64(hi);
   int rc = ensure_primes(std::max<uint32_t>(sq, 7u), err);
   if (rc) return rc;
-
   const auto upto = [&](uint64_t v) { return count_primes_le(v, false); };
   const auto below = [&](uint64_t v) { return count_primes_le(v, true); };
-  const uint32_t n_total = upto(sq);
-  const uint32_t n_small = std::min(below(small_limit_), n_total);
-  // medium primes must fit the shared-memory state area; the rest go to buckets
-  const uint32_t n_med = std::max(n_small, std::min({ below(big_limit_), n_total, n_small + state_cap_ }));
-  // beyond the shared state and below big_limit_: direct tier (no state)
-  const uint32_t n_dir = std::max(n_med, std::min(below(big_limit_), n_total));
-  const bool use_buckets = n_dir < n_total;
+  p.n_total = upto(sq);
+  p.n_small = std::min(below(small_limit_), p.n_total);
+  // medium primes must fit the shared-memory state area
+  p.n_med = std::max(p.n_small, std::min({ below(big_limit_), p.n_total, p.n_small + state_cap_ }));
+  // beyond the shared state and below big_limit_: direct tier (no state);
+  // the rest go to buckets
+  p.n_dir = std::max(p.n_med, std::min(below(big_limit_), p.n_total));
+  p.buckets = p.n_dir < p.n_total;
   // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
-  const uint32_t n_sweep_end = std::max(n_dir, std::min(below(sweep_limit_), n_total));
+  p.n_sweep_end = std::max(p.n_dir, std::min(below(sweep_limit_), p.n_total));
+  p.step = p.buckets ? window_ : (cfg_.segments_per_launch ? cfg_.segments_per_launch : p.nseg);
+  return PSG_OK;
+}
+
+int Engine::run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
+                cudaStream_t st, std::string& err) {
+  RangePlan p;
+  int rc = plan_range(lo, hi, p, err);
+  if (rc) return rc;
+  return run_windows(p, kinds, dev_counts, st, 0, p.windows(), err);
+}
+
+// Launches [w0, w0 + nw) of a planned range: one sieve launch per window of
+// p.step segments, each preceded by its bucket fill when the range has big
+// primes. Counts are added to dev_counts.
+int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
+                        cudaStream_t st, uint64_t w0, uint64_t nw, std::string& err) {
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  const uint64_t nseg = p.nseg, seg_low0 = p.seg_low0, step = p.step;
+  const bool use_buckets = p.buckets;
+  int rc;
   if (use_buckets) {
-    rc = ensure_buckets(n_dir, n_sweep_end, n_total, err);
+    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, err);
     if (rc) return rc;
   }
 
   SieveArgs a;
   fill_common_args(a);
-  a.lo = lo; a.hi = hi;
-  a.n_small = n_small;
-  a.n_primes = n_med;
-  a.n_direct = n_dir;
+  a.lo = p.lo; a.hi = p.hi;
+  a.n_small = p.n_small;
+  a.n_primes = p.n_med;
+  a.n_direct = p.n_dir;
   a.kinds = kinds;
   a.counts = dev_counts;
   const bool all = (kinds & ~1u) != 0;
 
-  const uint64_t step = use_buckets ? window_
-                      : (cfg_.segments_per_launch ? cfg_.segments_per_launch : nseg);
-  for (uint64_t s0 = 0; s0 < nseg; s0 += step) {
+  const uint64_t s_first = w0 * step;
+  const uint64_t s_last = std::min<uint64_t>(nseg, (w0 + nw) * step);
+  for (uint64_t s0 = s_first; s0 < s_last; s0 += step) {
     const uint64_t ns = std::min<uint64_t>(step, nseg - s0);
     const uint64_t win_low = seg_low0 + s0 * span;
     a.seg_low0 = win_low;

@@ -12,6 +12,7 @@
 #include <vector>
 #include <mutex>
 #include <cuda_runtime.h>
+#include "batch_types.hpp"
 
 namespace psg {
 
@@ -36,14 +37,23 @@ struct RangeQuery {
 
 struct SieveArgs;
 struct BatchArgs;
-struct BatchRange;
-struct BatchItem;
 
 // floor(sqrt(x))
 uint32_t isqrt_u64(uint64_t x);
 // The primes 2, 3, 5 and the k-tuplets containing them (not representable
 // in the wheel-30 bit array): counts added to out[kind] when start <= 5.
 void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]);
+
+// Prime tiers and launch geometry of one range [lo, hi] (lo >= 7):
+// primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
+// [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
+// n_sweep_end); sieve launches of `step` segments.
+struct RangePlan {
+  uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;
+  uint32_t n_small = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
+  bool buckets = false;
+  uint64_t windows() const { return (nseg + step - 1) / step; }
+};
 
 struct KernelStat {
   const char* name;
@@ -79,6 +89,30 @@ public:
   size_t batch_bucket_ranges() const { return batch_bucket_ranges_; }
   size_t batch_items() const { return batch_items_; }
 
+  // Tiers of [lo, hi] (lo >= 7) and launches of its windows [w0, w0 + nw);
+  // counts added to dev_counts on st. The bucket storage is shared: windows
+  // of different ranges must not overlap in time.
+  int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err);
+  int run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
+                  cudaStream_t st, uint64_t w0, uint64_t nw, std::string& err);
+
+  // Batch-kernel building blocks (also used by the request server):
+  // tiers of [lo, hi] for the persistent kernel (false: needs the bucket
+  // path), its stripes as work items, and one launch over device items.
+  bool batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r, double& seg_cost);
+  uint64_t range_segments(const BatchRange& r) const;
+  uint64_t append_stripes(uint32_t k, const BatchRange& r, double seg_cost, uint64_t s0, uint64_t max_seg,
+                          std::vector<BatchItem>& items, std::vector<double>& cost) const;
+  static void sort_items(std::vector<BatchItem>& items, const std::vector<double>& cost);
+  int launch_items(const BatchRange* d_ranges, const BatchItem* d_items, uint32_t n_items,
+                   unsigned long long* d_rows, uint32_t* d_queue, cudaStream_t st, std::string& err);
+  // Bucket-list overflow flag (device) and the response to it: lists grow
+  // and the next windows are planned again.
+  uint32_t* overflow_flag() { return d_overflow_; }
+  void grow_bucket_lists() { overflow_retries_++; cap_scale_ *= 2.0; bucket_first_ = bucket_mid_ = bucket_last_ = 0; }
+  // Estimated bucket storage of a planned range (bytes).
+  size_t bucket_bytes(const RangePlan& p) const;
+
   // Make sure the sieving-prime table covers sqrt(stop) (host work + upload).
   int prepare(uint64_t stop, std::string& err);
 
@@ -110,7 +144,7 @@ private:
   uint32_t count_primes_le(uint64_t v, bool strict);
   uint32_t count_primes_upper(uint64_t v) const;   // >= table primes <= v, no device read
   void fill_common_args(SieveArgs& a) const;
-  cudaError_t launch_batch(const BatchArgs& b);
+  cudaError_t launch_batch(const BatchArgs& b, cudaStream_t st);
   double approx_prime(uint32_t i) const;
   double inv_prefix(uint32_t i) const;   // ~ sum of 1/p over table primes [0, i)
   uint32_t approx_count_below(uint64_t v) const;

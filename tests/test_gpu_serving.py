@@ -1,0 +1,62 @@
+"""GPU: the request server (psg_server_*): continuous batching of count
+requests from the serving distribution. Every result equals the per-range
+count (psg_count) of the same request, whether the request ran alone on an
+idle server or mixed with many others on a loaded one; admission refuses a
+request whose bucket storage exceeds the HBM budget."""
+import random
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(psg, n, rate, seed=1):
+    # the serving distribution with lengths capped at 2^30 to bound test time
+    return psg.serving_workload(n, rate, seed=seed, len_log2=(12.0, 30.0))
+
+
+def test_server_alone_equals_in_mix(psg, ctx):
+    reqs, _ = _requests(psg, 120, 1000.0)
+    with psg.Server(ctx) as srv:
+        alone = []
+        for a, b, k in reqs:
+            counts, lat = srv.wait(srv.submit(a, b, k))
+            assert lat >= 0
+            alone.append(counts)
+        # all at once: every request shares steps with the others
+        mixed, lats = srv.replay(reqs, [0.0] * len(reqs))
+        st = srv.stats()
+    assert mixed == alone
+    assert st["completed"] == 2 * len(reqs)
+    assert st["bucket_requests"] > 0 and st["batch_requests"] > 0
+    for (a, b, k), got in random.Random(5).sample(list(zip(reqs, alone)), 25):
+        assert got == ctx.count(a, b, k), (a, b, k)
+
+
+def test_server_poisson_replay(psg, ctx):
+    reqs, arrivals = _requests(psg, 200, 2000.0, seed=11)
+    with psg.Server(ctx) as srv:
+        counts, lats = srv.replay(reqs, arrivals)
+    assert len(lats) == len(reqs) and min(lats) > 0
+    for (a, b, k), got in list(zip(reqs, counts))[::8]:
+        assert got == ctx.count(a, b, k), (a, b, k)
+
+
+def test_server_trivial_requests(psg, ctx):
+    with psg.Server(ctx) as srv:
+        cases = [(10, 5, 63), (0, 0, 63), (0, 6, 63), (2, 3, 1), (0, 100, 0), (3, 5, 2),
+                 (2 ** 64 - 1, 2 ** 64 - 1, 63), (0, 10 ** 6, 63)]
+        ids = [srv.submit(a, b, k) for a, b, k in cases]
+        for (a, b, k), i in zip(cases, ids):
+            assert srv.wait(i)[0] == ctx.count(a, b, k), (a, b, k)
+
+
+def test_server_refuses_over_hbm_budget(psg, ctx):
+    with psg.Server(ctx, hbm_budget=1 << 20) as srv:
+        big = srv.submit(10 ** 18, 10 ** 18 + 10 ** 10, 1)      # needs bucket lists
+        small = srv.submit(10 ** 9, 10 ** 9 + 10 ** 6, 1)       # batch kernel only
+        with pytest.raises(psg.PsgError) as e:
+            srv.wait(big)
+        assert e.value.status == 4 and "HBM budget" in str(e.value)
+        assert srv.wait(small)[0] == ctx.count(10 ** 9, 10 ** 9 + 10 ** 6, 1)
+        assert srv.stats()["refused"] == 1
