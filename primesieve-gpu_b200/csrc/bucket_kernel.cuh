@@ -35,9 +35,11 @@ struct BucketArgs {
   uint32_t seg_magic;         // floor(2^32 / seg_bytes) + 1 (segment index)
   uint32_t seg_shift;         // log2(seg_bytes) when it is a power of two
   uint32_t tile_steps;        // generate steps per warp between bin flushes
+  uint32_t wheel_tab[16];     // per class: bits, corr (wheel walk)
   const uint32_t* primes;
   const uint64_t* recip;
-  const uint32_t* chunk_begin;  // [CTAs + 1] prime index range per CTA
+  const uint32_t* chunk_begin;  // [CTAs + 1] group-walk prime range per CTA
+  const uint32_t* thread_chunk; // [CTAs + 1] thread-walk prime range per CTA
   uint32_t list_base;         // list of CTA 0 (the sweep kernel's lists come first)
   uint32_t num_lists;         // lists per segment, all kernels
   const uint32_t* list_off;   // [num_lists] entry offset inside a segment region
@@ -71,30 +73,59 @@ __device__ __forceinline__ uint32_t seg_of(uint32_t b, uint32_t seg_bytes, uint3
 // ever dropped whatever the distribution. After tile_steps steps per warp the
 // CTA copies every bin to the end of its segment's HBM list, 8 lanes per bin,
 // as one contiguous run (HBM sees whole sectors, not scattered 4-byte writes).
+// Primes with few multiples in a window (the CTA's thread_chunk range) are
+// walked one thread per prime through all 8 wheel classes (the medium tier's
+// wheel walk), so that locating a prime costs one lane, not eight; they
+// stream through shared memory in chunks of one prime per thread.
 // (A one-prime-per-warp walk emitting 32 consecutive multiples per step with
 // one rank atomic per segment run measured slower on B200: 42-47 ms against
 // 38 ms per pass on [1e15, 1e15+1e11].)
 constexpr uint32_t kBinCap = 32;          // bin slots per segment
 constexpr uint32_t kBinStride = 33;       // odd stride: bins start on different banks
 
-// smem: cnt[W] (entries of the tile per segment, may exceed kBinCap)
+// smem: thread-walk prime chunks rbuf[2][kChunk] (u64), pbuf[2][kChunk] |
+//       cnt[W] (entries of the tile per segment, may exceed kBinCap) |
 //       gcnt[W] (entries already in the HBM list) | bins[W][kBinStride]
+constexpr uint32_t kChunk = 1024;         // thread-walk primes per chunk (= threads)
+constexpr size_t kChunkBytes = 2ull * kChunk * (8 + 4);
+constexpr size_t kFillBytesPerSegment = (2 + kBinStride) * 4;
 constexpr size_t fill_smem_bytes(uint32_t W) {
-  return (size_t) W * (2 + kBinStride) * 4;
+  return kChunkBytes + (size_t) W * kFillBytesPerSegment;
 }
+
+// 4- and 8-byte asynchronous global->shared copies (zero-filled when
+// src_bytes is 0; the source address is then not read).
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n"
+               :: "r"((uint32_t) __cvta_generic_to_shared(dst)), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n"
+               :: "r"((uint32_t) __cvta_generic_to_shared(dst)), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
 
 template <int BLOCK, bool POW2>
 __global__ void __launch_bounds__(BLOCK, 1)
 bucket_fill_kernel(const __grid_constant__ BucketArgs a)
 {
+  static_assert(BLOCK == (int) kChunk, "one thread-walk prime per thread and chunk");
   constexpr uint32_t NWARPS = BLOCK / 32;
   extern __shared__ uint32_t smem_u32[];
   const uint32_t W = a.win_segments;
-  uint32_t* const cnt = smem_u32;                // [W]
+  uint64_t* const rbuf = reinterpret_cast<uint64_t*>(smem_u32);  // [2][kChunk]
+  uint32_t* const pbuf = smem_u32 + 4 * kChunk;  // [2][kChunk]
+  uint32_t* const cnt = pbuf + 2 * kChunk;       // [W]
   uint32_t* const gcnt = cnt + W;                // [W]
   uint32_t* const bins = gcnt + W;               // [W][kBinStride]
+  __shared__ uint32_t wheel_tab[16];
+  __shared__ uint32_t s_total;                   // entries in the bins since the last flush
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-  for (uint32_t i = tid; i < 2 * W; i += BLOCK) smem_u32[i] = 0;
+  for (uint32_t i = tid; i < 2 * W; i += BLOCK) cnt[i] = 0;
+  if (tid < 16) wheel_tab[tid] = a.wheel_tab[tid];
+  if (tid == 0) s_total = 0;
   __syncthreads();
 
   const uint32_t list = a.list_base + blockIdx.x;
@@ -107,13 +138,15 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   const uint64_t stride = a.seg_stride;
   const uint32_t lo = a.chunk_begin[blockIdx.x];
   const uint32_t hi = a.chunk_begin[blockIdx.x + 1];
+  const uint32_t t_lo = a.thread_chunk[blockIdx.x];
+  const uint32_t t_hi = a.thread_chunk[blockIdx.x + 1];
   const uint32_t steps = a.tile_steps;
   constexpr uint32_t kFull = 0xffffffffu;
   constexpr uint32_t kDone = 0xffffffffu;
   const uint32_t g = lane >> 3;
   const uint32_t Q = cofactor_class(lane & 7u);
 
-  // emit one entry per valid lane into its segment's bin (or its HBM list)
+  // emit one entry into its segment's bin (or straight into its HBM list)
   auto put = [&](uint32_t sg, uint32_t r, uint32_t e) {
     if (r < kBinCap) {
       bins[sg * kBinStride + r] = e;
@@ -126,72 +159,129 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
     if (POW2) { bo = b & (seg_bytes - 1u); return b >> shift; }
     return seg_of(b, seg_bytes, magic, bo);
   };
-
-  // ---- this lane's progression
-  uint32_t b = kDone, p = 0, ebit = 0;
-  uint32_t group = warp;                  // next group of 4 primes of this warp
-  bool warp_done = false;
-  uint32_t p_nx = 0;                      // prefetched prime of the next group
-  uint64_t r_nx = 0;
-  {
-    const uint32_t idx = lo + group * 4u + g;
-    if (idx < hi) { p_nx = a.primes[idx]; r_nx = a.recip[idx]; }
-  }
-
-  for (;;) {
-    // ---- 1. generate: tile_steps steps per warp into the bins
-    for (uint32_t step = 0; step < steps && !warp_done; step++) {
-      if (__ballot_sync(kFull, b != kDone) == 0) {
-        const uint32_t base = lo + group * 4u;
-        if (base >= hi) { warp_done = true; break; }
-        group += NWARPS;
-        const uint32_t idx = base + g;
-        const uint32_t p_cur = p_nx;
-        const uint64_t r_cur = r_nx;
-        {
-          const uint32_t nidx = lo + group * 4u + g;
-          if (nidx < hi) { p_nx = a.primes[nidx]; r_nx = a.recip[nidx]; }
-        }
-        if (idx < hi) {
-          p = p_cur;
-          uint64_t d; uint32_t c0;
-          first_multiple(a.win_low, p, r_cur, d, c0);
-          const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
-          const uint64_t b64 = (d + (uint64_t) k * p) / 30u;   // byte index in window
-          if (b64 < win_bytes) b = (uint32_t) b64;
-          ebit = residue_to_bit((Q * (p % 30u)) % 30u);
-        }
-      }
-      if (b != kDone) {
-        uint32_t bo;
-        const uint32_t sg = split_b(b, bo);
-        put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ebit);
-        // p >= win_bytes - b: no further hit (also keeps b + p from wrapping)
-        b = (p >= win_bytes - b) ? kDone : b + p;
-      }
-    }
-    const int more = __syncthreads_or(warp_done ? 0 : 1);
-
-    // ---- 2. copy every bin to the end of its HBM list: 8 lanes per bin
-    {
-      const uint32_t q = lane >> 3, j = lane & 7u;
-      for (uint32_t s0 = warp * 4u; s0 < W; s0 += NWARPS * 4u) {   // warp-uniform trip count
-        const uint32_t sg = s0 + q;
-        const bool valid = sg < W;
-        const uint32_t c = valid ? cnt[sg] : 0u;
-        const uint32_t n = min(c, kBinCap);
-        const uint32_t base = valid ? gcnt[sg] : 0u;
-        const uint32_t room = base < cap ? cap - base : 0u;
-        const uint32_t nw = min(n, room);
-        const uint32_t* src = bins + sg * kBinStride;
-        uint32_t* dst = out + (uint64_t) sg * stride + base;
-        for (uint32_t i = j; i < nw; i += 8u) dst[i] = src[i];
-        __syncwarp();
-        if (valid && j == 0) { gcnt[sg] = base + n; cnt[sg] = 0; }
-      }
+  // copy every bin to the end of its HBM list, 8 lanes per bin (all threads;
+  // the bins must be complete, i.e. after a barrier)
+  auto flush = [&]() {
+    const uint32_t q = lane >> 3, j = lane & 7u;
+    for (uint32_t s0 = warp * 4u; s0 < W; s0 += NWARPS * 4u) {   // warp-uniform trip count
+      const uint32_t sg = s0 + q;
+      const bool valid = sg < W;
+      const uint32_t c = valid ? cnt[sg] : 0u;
+      const uint32_t n = min(c, kBinCap);
+      const uint32_t base = valid ? gcnt[sg] : 0u;
+      const uint32_t room = base < cap ? cap - base : 0u;
+      const uint32_t nw = min(n, room);
+      const uint32_t* src = bins + sg * kBinStride;
+      uint32_t* dst = out + (uint64_t) sg * stride + base;
+      for (uint32_t i = j; i < nw; i += 8u) dst[i] = src[i];
+      __syncwarp();
+      if (valid && j == 0) { gcnt[sg] = base + n; cnt[sg] = 0; }
     }
     __syncthreads();
-    if (!more) break;
+  };
+
+  // ---- phase 1: group walk over primes [lo, hi), tiles of `steps` steps
+  {
+    uint32_t b = kDone, p = 0, ebit = 0;    // this lane's progression
+    uint32_t group = warp;                  // next group of 4 primes of this warp
+    bool warp_done = lo >= hi;
+    uint32_t p_nx = 0;                      // prefetched prime of the next group
+    uint64_t r_nx = 0;
+    {
+      const uint32_t idx = lo + group * 4u + g;
+      if (idx < hi) { p_nx = a.primes[idx]; r_nx = a.recip[idx]; }
+    }
+    for (;;) {
+      for (uint32_t step = 0; step < steps && !warp_done; step++) {
+        if (__ballot_sync(kFull, b != kDone) == 0) {
+          const uint32_t base = lo + group * 4u;
+          if (base >= hi) { warp_done = true; break; }
+          group += NWARPS;
+          const uint32_t idx = base + g;
+          const uint32_t p_cur = p_nx;
+          const uint64_t r_cur = r_nx;
+          {
+            const uint32_t nidx = lo + group * 4u + g;
+            if (nidx < hi) { p_nx = a.primes[nidx]; r_nx = a.recip[nidx]; }
+          }
+          if (idx < hi) {
+            p = p_cur;
+            uint64_t d; uint32_t c0;
+            first_multiple(a.win_low, p, r_cur, d, c0);
+            const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+            const uint64_t b64 = (d + (uint64_t) k * p) / 30u;   // byte index in window
+            if (b64 < win_bytes) b = (uint32_t) b64;
+            ebit = residue_to_bit((Q * (p % 30u)) % 30u);
+          }
+        }
+        if (b != kDone) {
+          uint32_t bo;
+          const uint32_t sg = split_b(b, bo);
+          put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ebit);
+          // p >= win_bytes - b: no further hit (also keeps b + p from wrapping)
+          b = (p >= win_bytes - b) ? kDone : b + p;
+        }
+      }
+      const int more = __syncthreads_or(warp_done ? 0 : 1);
+      flush();
+      if (!more) break;
+    }
+  }
+
+  // ---- phase 2: thread walk over primes [t_lo, t_hi), one prime per thread
+  // and chunk; the chunks stream through shared memory (cp.async, double
+  // buffered), the bins are flushed when they may be getting full
+  if (t_lo < t_hi) {
+    const uint32_t nchunk = (t_hi - t_lo + kChunk - 1) / kChunk;
+    const uint32_t flush_at = (uint32_t) (0.45f * (float) kBinCap * (float) W);
+    auto issue = [&](uint32_t k) {
+      const uint32_t i = t_lo + k * kChunk + tid;
+      const bool in = i < t_hi;
+      const uint32_t src = in ? i : t_lo;         // a valid address even when zero-filling
+      cp_async4(pbuf + (k & 1u) * kChunk + tid, a.primes + src, in ? 4u : 0u);
+      cp_async8(rbuf + (k & 1u) * kChunk + tid, a.recip + src, in ? 8u : 0u);
+      cp_async_commit();
+    };
+    issue(0);
+    for (uint32_t k = 0; k < nchunk; k++) {
+      if (k + 1 < nchunk) { issue(k + 1); cp_async_wait<1>(); }
+      else cp_async_wait<0>();
+      __syncthreads();                            // chunk k complete for every thread
+      const uint32_t pc = pbuf[(k & 1u) * kChunk + tid];
+      const uint64_t rc = rbuf[(k & 1u) * kChunk + tid];
+      uint32_t emitted = 0;
+      if (pc != 0) {
+        uint64_t d; uint32_t c0;
+        first_multiple(a.win_low, pc, rc, d, c0);
+        uint32_t j = first_class_ge(c0);
+        const uint64_t b64 = (d + (uint64_t) (cofactor_class(j) - c0) * pc) / 30u;
+        if (b64 < win_bytes) {
+          uint32_t tb = (uint32_t) b64;
+          const uint32_t tpd = pc / 30u;
+          const uint32_t cls = residue_to_bit(pc - 30u * tpd);
+          const uint32_t tbits = wheel_tab[2 * cls], tcorr = wheel_tab[2 * cls + 1];
+          do {
+            uint32_t bo;
+            const uint32_t sg = split_b(tb, bo);
+            const uint32_t sh = 3u * j;
+            put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ((tbits >> sh) & 7u));
+            emitted++;
+            // tb < 2^31 and the step < 2^30: no wrap
+            tb += tpd * ((kGapPacked >> sh) & 7u) + ((tcorr >> sh) & 7u);
+            j = (j + 1u) & 7u;
+          } while (tb < win_bytes);
+        }
+      }
+      emitted = __reduce_add_sync(kFull, emitted);
+      if (lane == 0 && emitted) atomicAdd(&s_total, emitted);
+      __syncthreads();                            // chunk k consumed; s_total complete
+      const bool full = s_total >= flush_at || k + 1 == nchunk;
+      if (full) {
+        flush();
+        if (tid == 0) s_total = 0;
+        __syncthreads();
+      }
+    }
   }
 
   uint32_t written = 0;

@@ -290,7 +290,7 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   // the bucket fill kernel keeps one bin per window segment in shared memory
   // and indexes a window with 32-bit byte offsets
   const size_t fill_smem_max = (size_t) prop_.sharedMemPerBlockOptin;
-  window_ = std::min<uint32_t>(window_, (uint32_t) (fill_smem_max / fill_smem_bytes(1)));
+  window_ = std::min<uint32_t>(window_, (uint32_t) ((fill_smem_max - kChunkBytes) / kFillBytesPerSegment));
   window_ = std::min<uint32_t>(window_, (uint32_t) ((1ull << 31) / seg_bytes_));
   window_ = std::max<uint32_t>(window_, 1u);
   seg_pow2_ = (seg_bytes_ & (seg_bytes_ - 1u)) == 0;
@@ -610,25 +610,35 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
   if (nfill) {
     fill_ctas = std::max<uint32_t>(1, std::min<uint32_t>(lists_, nfill));
     const double win_span = span * (8.0 / 30.0) * (double) window_;
-    const double setup = 8.0;      // per-window setup of a prime, in entries
-    // chunk boundaries for equal (setup + hits) work: binary search on the
-    // monotone cost over the 1/p prefix table
+    // per-window setup of a prime in entries: 8 lanes in the group walk,
+    // one in the thread walk
+    const double setup_group = 8.0;
+    // group walk: primes [mid, t_end), chunks of equal (setup + hits) work
+    // by binary search on the monotone cost over the 1/p prefix table;
+    // thread walk: primes [t_end, last) (a few multiples each, cost per
+    // prime nearly uniform), equal counts per CTA
+    const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), mid), last);
     const double s_mid = inv_prefix(mid);
-    const auto cost = [&](uint32_t i) { return setup * (double) (i - mid) + win_span * (inv_prefix(i) - s_mid); };
-    const double total = cost(last);
-    begin.assign(fill_ctas + 1, last);
+    const auto cost = [&](uint32_t i) { return setup_group * (double) (i - mid) + win_span * (inv_prefix(i) - s_mid); };
+    const double total = cost(t_end);
+    begin.assign(2 * (fill_ctas + 1), t_end);
     begin[0] = mid;
     for (uint32_t l = 1; l < fill_ctas; l++) {
       const double target = total * (double) l / (double) fill_ctas;
-      uint32_t x = begin[l - 1], y = last;       // smallest i in [x, y] with cost(i) >= target
+      uint32_t x = begin[l - 1], y = t_end;      // smallest i in [x, y] with cost(i) >= target
       while (x < y) {
         const uint32_t m = x + (y - x) / 2;
         if (cost(m) >= target) y = m; else x = m + 1;
       }
       begin[l] = x;
     }
+    uint32_t* tchunk = begin.data() + fill_ctas + 1;
+    for (uint32_t l = 0; l <= fill_ctas; l++)
+      tchunk[l] = t_end + (uint32_t) ((uint64_t) (last - t_end) * l / fill_ctas);
     std::vector<double> mu(fill_ctas, 0.0);
-    for (uint32_t c = 0; c < fill_ctas; c++) mu[c] = per_seg * (inv_prefix(begin[c + 1]) - inv_prefix(begin[c]));
+    for (uint32_t c = 0; c < fill_ctas; c++)
+      mu[c] = per_seg * (inv_prefix(begin[c + 1]) - inv_prefix(begin[c]) +
+                         inv_prefix(tchunk[c + 1]) - inv_prefix(tchunk[c]));
     for (uint32_t c = 0; c < fill_ctas; c++) add_list(mu[c]);
   }
   const uint32_t lists = sweep_ctas + fill_ctas;
@@ -654,7 +664,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     cudaFree(d_list_off_); cudaFree(d_list_cap_); cudaFree(d_chunk_begin_);
     PSG_CUDA(cudaMalloc(&d_list_off_, (lists + 1) * sizeof(uint32_t)));
     PSG_CUDA(cudaMalloc(&d_list_cap_, (lists + 1) * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&d_chunk_begin_, (lists + 1) * sizeof(uint32_t)));
+    PSG_CUDA(cudaMalloc(&d_chunk_begin_, 2 * (lists + 1) * sizeof(uint32_t)));
     lists_cap_ = lists + 1;
   }
   if (nsweep > sweep_state_cap_) {
@@ -666,7 +676,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
   PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
   if (fill_ctas)
-    PSG_CUDA(cudaMemcpyAsync(d_chunk_begin_, begin.data(), (fill_ctas + 1) * sizeof(uint32_t),
+    PSG_CUDA(cudaMemcpyAsync(d_chunk_begin_, begin.data(), 2 * (fill_ctas + 1) * sizeof(uint32_t),
                              cudaMemcpyHostToDevice, stream_));
   PSG_CUDA(cudaStreamSynchronize(stream_));
   seg_stride_ = stride;
@@ -861,9 +871,14 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.seg_shift = seg_shift_;
         // steps per tile: a bin expects at most ~45% of its slots per tile
         b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (0.45 * kBinCap * (double) ns / kBucketBlock));
+        for (uint32_t c = 0; c < 8; c++) {
+          b.wheel_tab[2 * c] = wheel_bits_packed(c);
+          b.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
+        }
         b.primes = d_primes_;
         b.recip = d_recip_;
         b.chunk_begin = d_chunk_begin_;
+        b.thread_chunk = d_chunk_begin_ + fill_ctas_ + 1;
         b.list_base = sweep_ctas_;
         b.num_lists = active_lists_;
         b.list_off = d_list_off_;

@@ -148,6 +148,9 @@ private:
   double approx_prime(uint32_t i) const;
   double inv_prefix(uint32_t i) const;   // ~ sum of 1/p over table primes [0, i)
   uint32_t approx_count_below(uint64_t v) const;
+  // big primes from this value on have at most ~8 multiples in a window of
+  // w segments: the fill kernel walks them one lane per prime
+  uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_; }
   int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
