@@ -37,6 +37,11 @@ METRIC = "integers sieved/s, exact pi/k-tuplet counts: batched vs per-range; p50
 UNIT = "integers/s"
 WORKLOAD = "count primes in [1e15, 1e15+1e11] (sieving primes <= 3.16e7, bucket sieve)"
 GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
+# ncu, [1e15, 1e15+2e9] (one window, 167,958,746 bucket entries):
+# fill kernel 614.888960 MB written + 71.998976 MB read, sieve kernel
+# 662.998016 MB read + 5.111552 MB written
+FILL_DRAM_BYTES_PER_ENTRY = (614.888960e6 + 71.998976e6) / 167958746
+SIEVE_DRAM_BYTES_PER_ENTRY = (662.998016e6 + 5.111552e6) / 167958746
 
 
 def env_rank():
@@ -269,13 +274,20 @@ def main():
     crossings = crossing_count(b)
     sieve_rate = crossings / max(sieve_ms * 1e-3, 1e-12)
     dominant = "bucket_fill_kernel" if fill_ms > sieve_ms else "sieve_count_kernel"
+    # DRAM traffic per launch: bytes per bucket entry from one ncu capture of
+    # each kernel on [1e15, 1e15+2e9] (one 509-segment window, 167,958,746
+    # entries), scaled by this launch's entries
+    entries_per_launch = entries_per_pass / max(fill_l, 1)
+    fill_traffic = FILL_DRAM_BYTES_PER_ENTRY * entries_per_launch
+    sieve_traffic = SIEVE_DRAM_BYTES_PER_ENTRY * entries_per_launch
     roof_fill = {"kernel": "bucket_fill_kernel", "bound": "hbm", "achieved": fill_gbs, "peak": hbm_peak,
-                 "unit": "GB/s", "frac": fill_gbs / hbm_peak, "traffic": None,
+                 "unit": "GB/s", "frac": fill_gbs / hbm_peak, "traffic": fill_traffic,
+                 "traffic_source": "ncu dram__bytes_read+write per entry on a one-window case, scaled",
                  "algorithmic_bytes_per_launch": fill_bytes / max(fill_l, 1),
                  "avg_launch_ms": fill_ms / max(fill_l, 1), "peak_source": peak_src}
     roof_sieve = {"kernel": "sieve_count_kernel", "bound": "smem_atomic", "achieved": sieve_rate / 1e9,
                   "peak": smem_rate / 1e9, "unit": "Gatomic/s", "frac": sieve_rate / max(smem_rate, 1),
-                  "traffic": None, "crossings_per_pass": crossings,
+                  "traffic": sieve_traffic, "crossings_per_pass": crossings,
                   "bucket_entries_applied_per_pass": entries_per_pass,
                   "avg_launch_ms": sieve_ms / max(sieve_l, 1),
                   "peak_source": "measured in-run (random-address smem atomicAnd probe)"}

@@ -36,6 +36,8 @@ void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6])
 namespace {
 
 constexpr int kBucketBlock = 1024;
+constexpr double kSetupGroup = 8.0;     // fill-chunk cost of locating a group-walk prime (entries)
+constexpr double kSetupThread = 4.0;    // ... of a thread-walk prime
 constexpr int kSweepWarps = 16;     // sweep CTA = 512 threads
 constexpr int kSweepK = 16;         // sieving primes per sweep lane
 
@@ -612,29 +614,33 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     const double win_span = span * (8.0 / 30.0) * (double) window_;
     // per-window setup of a prime in entries: 8 lanes in the group walk,
     // one in the thread walk
-    const double setup_group = 8.0;
-    // group walk: primes [mid, t_end), chunks of equal (setup + hits) work
-    // by binary search on the monotone cost over the 1/p prefix table;
-    // thread walk: primes [t_end, last) (a few multiples each, cost per
-    // prime nearly uniform), equal counts per CTA
+    // Per-window cost of a prime in entry units: its setup (8 lanes in the
+    // group walk, one in the thread walk) plus its entries. Group walk:
+    // primes [mid, t_end); thread walk: primes [t_end, last). Each range is
+    // cut into fill_ctas chunks of equal cost (binary search on the monotone
+    // cost over the 1/p prefix table); CTA c takes chunk c of both.
+    const double setup_group = kSetupGroup, setup_thread = kSetupThread;
     const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), mid), last);
-    const double s_mid = inv_prefix(mid);
-    const auto cost = [&](uint32_t i) { return setup_group * (double) (i - mid) + win_span * (inv_prefix(i) - s_mid); };
-    const double total = cost(t_end);
-    begin.assign(2 * (fill_ctas + 1), t_end);
-    begin[0] = mid;
-    for (uint32_t l = 1; l < fill_ctas; l++) {
-      const double target = total * (double) l / (double) fill_ctas;
-      uint32_t x = begin[l - 1], y = t_end;      // smallest i in [x, y] with cost(i) >= target
-      while (x < y) {
-        const uint32_t m = x + (y - x) / 2;
-        if (cost(m) >= target) y = m; else x = m + 1;
+    begin.assign(2 * (fill_ctas + 1), 0);
+    const auto cut = [&](uint32_t from, uint32_t to, double setup, uint32_t* bounds) {
+      const double s0 = inv_prefix(from);
+      const auto cost = [&](uint32_t i) { return setup * (double) (i - from) + win_span * (inv_prefix(i) - s0); };
+      const double total = cost(to);
+      bounds[0] = from;
+      bounds[fill_ctas] = to;
+      for (uint32_t l = 1; l < fill_ctas; l++) {
+        const double target = total * (double) l / (double) fill_ctas;
+        uint32_t x = bounds[l - 1], y = to;      // smallest i in [x, y] with cost(i) >= target
+        while (x < y) {
+          const uint32_t m = x + (y - x) / 2;
+          if (cost(m) >= target) y = m; else x = m + 1;
+        }
+        bounds[l] = x;
       }
-      begin[l] = x;
-    }
+    };
+    cut(mid, t_end, setup_group, begin.data());
     uint32_t* tchunk = begin.data() + fill_ctas + 1;
-    for (uint32_t l = 0; l <= fill_ctas; l++)
-      tchunk[l] = t_end + (uint32_t) ((uint64_t) (last - t_end) * l / fill_ctas);
+    cut(t_end, last, setup_thread, tchunk);
     std::vector<double> mu(fill_ctas, 0.0);
     for (uint32_t c = 0; c < fill_ctas; c++)
       mu[c] = per_seg * (inv_prefix(begin[c + 1]) - inv_prefix(begin[c]) +
