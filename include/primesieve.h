@@ -27,6 +27,42 @@
 extern "C" {
 #endif
 
+/* Element types of primesieve_generate_primes() / _generate_n_primes()
+ * (same names and values as the reference, include/primesieve.h:37-66). */
+enum {
+  SHORT_PRIMES,
+  USHORT_PRIMES,
+  INT_PRIMES,
+  UINT_PRIMES,
+  LONG_PRIMES,
+  ULONG_PRIMES,
+  LONGLONG_PRIMES,
+  ULONGLONG_PRIMES,
+  INT16_PRIMES,
+  UINT16_PRIMES,
+  INT32_PRIMES,
+  UINT32_PRIMES,
+  INT64_PRIMES,
+  UINT64_PRIMES
+};
+
+/* The primes inside [start, stop] as a malloc'd array of `type` elements
+ * (free with primesieve_free); *size = number of primes. NULL, *size = 0 and
+ * errno = EDOM on error (reference include/primesieve.h:68-81,
+ * src/api-c.cpp). The primes are extracted on the GPU. */
+void* primesieve_generate_primes(uint64_t start, uint64_t stop, size_t* size, int type);
+
+/* The first n primes >= start (reference include/primesieve.h:83-96). */
+void* primesieve_generate_n_primes(uint64_t n, uint64_t start, int type);
+
+/* n > 0: the nth prime > start; n = 0: the first prime > start; n < 0: the
+ * |n|th prime < start (reference include/primesieve.h:98-115). Located with
+ * exact GPU counts. PRIMESIEVE_ERROR + errno = EDOM on error. */
+uint64_t primesieve_nth_prime(int64_t n, uint64_t start);
+
+/* Frees an array of primesieve_generate_primes / _generate_n_primes. */
+void primesieve_free(void* primes);
+
 /* Count the primes / prime k-tuplets inside [start, stop], stop <= 2^64-1.
  * Reference: include/primesieve.h:130-170, src/api-c.cpp:143-225. */
 uint64_t primesieve_count_primes(uint64_t start, uint64_t stop);

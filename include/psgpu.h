@@ -111,6 +111,22 @@ int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t ki
 int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n,
                     uint64_t* counts);
 
+/* The primes in [start, stop], ascending. Replaces the reference's CPU prime
+ * extraction (src/CountPrintPrimes.cpp:187-259, store_primes in
+ * include/primesieve/StorePrimes.hpp): the GPU sieve keeps its segments as
+ * bitmaps and a GPU kernel turns them into values. *count gets the number
+ * of primes; up to `capacity` of them are written to out (host memory);
+ * PSG_ERR_LIMIT when capacity < *count (nothing is lost: call again). */
+int psg_generate_primes(psg_context* ctx, uint64_t start, uint64_t stop,
+                        uint64_t* out, size_t capacity, size_t* count);
+
+/* primesieve's nth_prime(n, start) (src/nthPrime.cpp:47-181): n > 0 the nth
+ * prime > start, n = 0 the first prime > start, n < 0 the |n|th prime
+ * < start. Exact GPU counts locate it; the last bracket is sieved as a
+ * bitmap. Errors (PSG_ERR_ARG / PSG_ERR_LIMIT) carry the reference's
+ * messages. */
+int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime);
+
 /* Build the sieving-prime table up to sqrt(stop) ahead of time. */
 int psg_prepare(psg_context* ctx, uint64_t stop);
 

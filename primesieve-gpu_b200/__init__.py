@@ -29,7 +29,7 @@ PSG_SYMBOLS = (
     "psg_set_profiling", "psg_kernel_stats", "psg_reset_kernel_stats", "psg_version",
     "psg_bucket_entries", "psg_measure_smem_atomic_rate", "psg_count_noalloc",
     "psg_server_start", "psg_server_submit", "psg_server_wait", "psg_server_replay",
-    "psg_server_get_stats", "psg_server_stop",
+    "psg_server_get_stats", "psg_server_stop", "psg_generate_primes", "psg_nth_prime",
 )
 
 
@@ -108,6 +108,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_server_get_stats.argtypes = [vp, ctypes.POINTER(PsgServerStats)]
     lib.psg_server_stop.argtypes = [vp]
     lib.psg_server_stop.restype = None
+    lib.psg_generate_primes.argtypes = [vp, u64, u64, U64P, sz, ctypes.POINTER(sz)]
+    lib.psg_nth_prime.argtypes = [vp, ctypes.c_int64, u64, U64P]
     for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
         fn = getattr(lib, "primesieve_count_" + name, None)
         if fn is not None:
@@ -192,6 +194,27 @@ class Context:
         out = (ctypes.c_uint64 * (6 * max(n, 1)))()
         _check(self._lib.psg_count_batch(self._h, arr, n, out))
         return [list(out[6 * i:6 * i + 6]) for i in range(n)]
+
+    def generate_primes(self, start: int, stop: int) -> List[int]:
+        """The primes in [start, stop] (psg_generate_primes)."""
+        n = ctypes.c_size_t(0)
+        cap = 0
+        for _ in range(2):
+            out = (ctypes.c_uint64 * max(cap, 1))()
+            st = self._lib.psg_generate_primes(self._h, start, stop, out, cap, ctypes.byref(n))
+            if st == 0:
+                return list(out[:n.value])
+            if st != 5:                        # PSG_ERR_LIMIT: capacity too small
+                _check(st)
+            cap = n.value
+        _check(st)
+        return []
+
+    def nth_prime(self, n: int, start: int = 0) -> int:
+        """primesieve's nth_prime(n, start) (psg_nth_prime)."""
+        p = ctypes.c_uint64(0)
+        _check(self._lib.psg_nth_prime(self._h, n, start, ctypes.byref(p)))
+        return p.value
 
     def prepare(self, stop: int) -> None:
         _check(self._lib.psg_prepare(self._h, stop))

@@ -1,4 +1,5 @@
-// api.cpp -- primesieve-compatible C and C++ counting API over the psg_* ABI.
+// api.cpp -- primesieve-compatible C and C++ API over the psg_* ABI:
+// counts, nth_prime and prime generation.
 //
 // Mirrors the reference's public counting API (src/api.cpp:48-118,
 // src/api-c.cpp:143-225) and its GPU API (src/gpu/GpuSieve.cpp:184-365):
@@ -12,6 +13,8 @@
 #include "../../include/psgpu.h"
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <cerrno>
 #include <iostream>
 #include <mutex>
@@ -85,6 +88,92 @@ uint64_t c_count(const char* name, uint64_t start, uint64_t stop, int kind) {
   }
 }
 
+// psg status -> primesieve_error with the engine's message (argument errors
+// keep the reference's wording, e.g. "nth_prime(n): abs(n) must be < start")
+[[noreturn]] void throw_status(int rc) {
+  g_last_error = psg_last_error();
+  if (rc == PSG_ERR_CUDA || rc == PSG_ERR_NO_DEVICE || rc == PSG_ERR_INTERNAL) reset_context_locked();
+  throw primesieve::primesieve_error(g_last_error.empty() ? psg_status_string(rc) : g_last_error);
+}
+
+psg_context* require_context_locked() {
+  psg_context* c = context_locked();
+  if (!c) throw primesieve::primesieve_error("GPU is not available: " + g_last_error);
+  return c;
+}
+
+void generate_locked(uint64_t start, uint64_t stop, std::vector<uint64_t>& out) {
+  psg_context* c = require_context_locked();
+  if (start > stop) return;
+  // capacity: an upper bound of pi(stop) - pi(start) first, the exact count
+  // if that was short
+  const double x = std::max(100.0, (double) stop);
+  size_t cap = (size_t) ((double) (stop - start) / (std::log(x) - 1.1) + 16.0);
+  for (int attempt = 0; attempt < 2; attempt++) {
+    const size_t old = out.size();
+    out.resize(old + cap);
+    size_t n = 0;
+    const int rc = psg_generate_primes(c, start, stop, out.data() + old, cap, &n);
+    if (rc == PSG_OK) { out.resize(old + n); return; }
+    out.resize(old);
+    if (rc != PSG_ERR_LIMIT) throw_status(rc);
+    cap = n;
+  }
+  throw primesieve::primesieve_error("generate_primes: inconsistent prime count");
+}
+
+uint64_t nth_prime_locked(int64_t n, uint64_t start) {
+  psg_context* c = require_context_locked();
+  uint64_t p = 0;
+  const int rc = psg_nth_prime(c, n, start, &p);
+  if (rc != PSG_OK) throw_status(rc);
+  return p;
+}
+
+template <typename T>
+void* c_generate(const char* name, uint64_t start, uint64_t stop, uint64_t n, bool first_n, size_t* size) {
+  try {
+    std::vector<T> v;
+    if (first_n) primesieve::generate_n_primes(n, start, &v);
+    else primesieve::generate_primes(start, stop, &v);
+    if (size) *size = v.size();
+    if (v.empty()) return nullptr;
+    T* out = static_cast<T*>(std::malloc(v.size() * sizeof(T)));
+    if (!out) throw std::bad_alloc();
+    std::copy(v.begin(), v.end(), out);
+    return out;
+  } catch (const std::exception& e) {
+    if (size) *size = 0;
+    std::cerr << name << ": " << e.what() << std::endl;
+    errno = EDOM;
+    return nullptr;
+  }
+}
+
+void* c_generate_typed(const char* name, uint64_t start, uint64_t stop, uint64_t n, bool first_n,
+                       size_t* size, int type) {
+  switch (type) {
+    case SHORT_PRIMES:     return c_generate<short>(name, start, stop, n, first_n, size);
+    case USHORT_PRIMES:    return c_generate<unsigned short>(name, start, stop, n, first_n, size);
+    case INT_PRIMES:       return c_generate<int>(name, start, stop, n, first_n, size);
+    case UINT_PRIMES:      return c_generate<unsigned int>(name, start, stop, n, first_n, size);
+    case LONG_PRIMES:      return c_generate<long>(name, start, stop, n, first_n, size);
+    case ULONG_PRIMES:     return c_generate<unsigned long>(name, start, stop, n, first_n, size);
+    case LONGLONG_PRIMES:  return c_generate<long long>(name, start, stop, n, first_n, size);
+    case ULONGLONG_PRIMES: return c_generate<unsigned long long>(name, start, stop, n, first_n, size);
+    case INT16_PRIMES:     return c_generate<int16_t>(name, start, stop, n, first_n, size);
+    case UINT16_PRIMES:    return c_generate<uint16_t>(name, start, stop, n, first_n, size);
+    case INT32_PRIMES:     return c_generate<int32_t>(name, start, stop, n, first_n, size);
+    case UINT32_PRIMES:    return c_generate<uint32_t>(name, start, stop, n, first_n, size);
+    case INT64_PRIMES:     return c_generate<int64_t>(name, start, stop, n, first_n, size);
+    case UINT64_PRIMES:    return c_generate<uint64_t>(name, start, stop, n, first_n, size);
+  }
+  if (size) *size = 0;
+  std::cerr << name << ": Invalid type parameter!" << std::endl;
+  errno = EDOM;
+  return nullptr;
+}
+
 int max_threads() {
   unsigned n = std::thread::hardware_concurrency();
   return n ? (int) n : 1;
@@ -109,6 +198,32 @@ std::array<uint64_t, 6> count_all(uint64_t start, uint64_t stop) {
   std::array<uint64_t, 6> out{};
   count_locked(start, stop, PSG_ALL_KINDS, out.data());
   return out;
+}
+
+uint64_t nth_prime(int64_t n, uint64_t start) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return nth_prime_locked(n, start);
+}
+
+void generate_primes_u64(uint64_t start, uint64_t stop, std::vector<uint64_t>& out) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  generate_locked(start, stop, out);
+}
+
+void generate_n_primes_u64(uint64_t n, uint64_t start, std::vector<uint64_t>& out) {
+  if (n == 0) return;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  // the nth prime >= start is the nth prime > start - 1
+  const uint64_t last = (start == 0) ? nth_prime_locked((int64_t) n, 0)
+                                     : nth_prime_locked((int64_t) n, start - 1);
+  generate_locked(start, last, out);
+}
+
+void check_element_type(const char* fn, int bits, bool is_signed, const char* name, uint64_t largest) {
+  const uint64_t max = is_signed ? ((1ull << (bits - 1)) - 1) : (bits >= 64 ? ~0ull : (1ull << bits) - 1);
+  if (largest > max)
+    throw primesieve_error(std::string(fn) + ": " + name + " is too narrow for generating primes up to " +
+                           std::to_string(largest));
 }
 
 uint64_t get_max_stop() { return ~(uint64_t) 0; }
@@ -275,6 +390,26 @@ int primesieve_count_all(uint64_t start, uint64_t stop, uint64_t counts[6]) {
     return -1;
   }
 }
+
+void* primesieve_generate_primes(uint64_t start, uint64_t stop, size_t* size, int type) {
+  return c_generate_typed("primesieve_generate_primes", start, stop, 0, false, size, type);
+}
+
+void* primesieve_generate_n_primes(uint64_t n, uint64_t start, int type) {
+  return c_generate_typed("primesieve_generate_n_primes", start, 0, n, true, nullptr, type);
+}
+
+uint64_t primesieve_nth_prime(int64_t n, uint64_t start) {
+  try {
+    return primesieve::nth_prime(n, start);
+  } catch (const std::exception& e) {
+    std::cerr << "primesieve_nth_prime: " << e.what() << std::endl;
+    errno = EDOM;
+    return PRIMESIEVE_ERROR;
+  }
+}
+
+void primesieve_free(void* primes) { std::free(primes); }
 
 uint64_t primesieve_get_max_stop(void) { return primesieve::get_max_stop(); }
 int primesieve_get_sieve_size(void) { return primesieve::get_sieve_size(); }

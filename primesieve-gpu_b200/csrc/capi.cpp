@@ -8,6 +8,7 @@
 #include "server.hpp"
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -15,6 +16,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 struct psg_context {
   psg::Engine engine;
@@ -238,6 +240,29 @@ int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n, uint64_
   std::lock_guard<std::mutex> lock(ctx->mu);
   std::string err;
   int rc = ctx->engine.count_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, counts, err);
+  return rc ? fail(rc, err) : PSG_OK;
+}
+
+int psg_generate_primes(psg_context* ctx, uint64_t start, uint64_t stop, uint64_t* out, size_t capacity,
+                        size_t* count) {
+  if (!ctx || !count || (capacity && !out)) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  std::vector<uint64_t> v;
+  int rc = ctx->engine.generate_primes(start, stop, v, err);
+  if (rc) return fail(rc, err);
+  *count = v.size();
+  std::copy(v.begin(), v.begin() + std::min(v.size(), capacity), out);
+  if (capacity < v.size())
+    return fail(PSG_ERR_LIMIT, "output capacity " + std::to_string(capacity) + " < " + std::to_string(v.size()) + " primes");
+  return PSG_OK;
+}
+
+int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime) {
+  if (!ctx || !prime) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  int rc = ctx->engine.nth_prime(n, start, *prime, err);
   return rc ? fail(rc, err) : PSG_OK;
 }
 

@@ -7,9 +7,10 @@
 // help src/app/help.cpp). Same option spellings, same output lines
 // ("Primes: N", "Twin primes: N", ...; a bare number with -q and a single
 // count; "Seconds: x.xxx" with --time, which is the default without -q).
-// Differences: every count runs on the GPU, all requested counts come from
-// one sieve pass, and the print / nth-prime / stress-test modes of the
-// reference are not part of this tool.
+// Also --nth-prime (main.cpp:256-290) and --print for primes (the primes
+// extracted on the GPU). Differences: everything runs on the GPU, all
+// requested counts come from one sieve pass; printing k-tuplets, RiemannR
+// and the stress test of the reference are not part of this tool.
 #include "../../../include/primesieve.hpp"
 #include "../../../include/primesieve/gpu.hpp"
 #include "calculator.hpp"
@@ -28,7 +29,7 @@ namespace {
 enum OptionId {
   OPT_COUNT, OPT_DIST, OPT_GPU, OPT_GPU_DEVICE, OPT_GPU_INFO, OPT_HELP,
   OPT_NUMBER, OPT_QUIET, OPT_SIZE, OPT_THREADS, OPT_TIME, OPT_VERSION,
-  OPT_NO_STATUS, OPT_UNSUPPORTED
+  OPT_NO_STATUS, OPT_NTH_PRIME, OPT_PRINT, OPT_UNSUPPORTED
 };
 enum Param { NO_PARAM, REQUIRED_PARAM, OPTIONAL_PARAM };
 
@@ -42,6 +43,8 @@ struct Options {
   bool time = false;
   bool help = false;
   bool version = false;
+  bool nth_prime = false;
+  bool print = false;
 };
 
 struct Parsed { std::string str, opt, val; };
@@ -68,9 +71,9 @@ const std::map<std::string, std::pair<OptionId, Param>>& option_map() {
     { "-v", { OPT_VERSION, NO_PARAM } }, { "--version", { OPT_VERSION, NO_PARAM } },
     { "--no-status", { OPT_NO_STATUS, NO_PARAM } },
     // reference modes outside the counting path
-    { "-p", { OPT_UNSUPPORTED, OPTIONAL_PARAM } }, { "--print", { OPT_UNSUPPORTED, OPTIONAL_PARAM } },
-    { "-n", { OPT_UNSUPPORTED, NO_PARAM } }, { "--nth-prime", { OPT_UNSUPPORTED, NO_PARAM } },
-    { "--nthprime", { OPT_UNSUPPORTED, NO_PARAM } },
+    { "-p", { OPT_PRINT, OPTIONAL_PARAM } }, { "--print", { OPT_PRINT, OPTIONAL_PARAM } },
+    { "-n", { OPT_NTH_PRIME, NO_PARAM } }, { "--nth-prime", { OPT_NTH_PRIME, NO_PARAM } },
+    { "--nthprime", { OPT_NTH_PRIME, NO_PARAM } },
     { "-R", { OPT_UNSUPPORTED, NO_PARAM } }, { "--RiemannR", { OPT_UNSUPPORTED, NO_PARAM } },
     { "--RiemannR-inverse", { OPT_UNSUPPORTED, NO_PARAM } },
     { "-S", { OPT_UNSUPPORTED, OPTIONAL_PARAM } }, { "--stress-test", { OPT_UNSUPPORTED, OPTIONAL_PARAM } },
@@ -171,6 +174,12 @@ Options parse(int argc, char** argv) {
       case OPT_TIME: opts.time = true; break;
       case OPT_VERSION: opts.version = true; break;
       case OPT_NO_STATUS: break;
+      case OPT_NTH_PRIME: opts.nth_prime = true; break;
+      case OPT_PRINT:                                     // CmdOptions.cpp:282-300
+        if (!o.val.empty() && eval_int(o) != 1)
+          fail("option '" + o.opt + "=" + o.val + "' is not supported: this build prints primes only");
+        opts.print = true;
+        break;
       case OPT_UNSUPPORTED:
         fail("option '" + o.opt + "' is not supported: this primesieve build counts "
              "primes and prime k-tuplets on the GPU only");
@@ -197,6 +206,10 @@ void help(int code) {
     "      --gpu-device=NUM       Use GPU device NUM, as listed by --gpu-info.\n"
     "      --gpu-info             Print the available GPU devices.\n"
     "  -h, --help                 Print this help menu.\n"
+    "  -n, --nth-prime            Find the nth prime, e.g. 100 -n finds the 100th\n"
+    "                             prime; with 2 numbers N START finds the nth\n"
+    "                             prime > START.\n"
+    "  -p, --print                Print the primes inside [START, STOP].\n"
     "  -q, --quiet                Quiet mode, prints less output.\n"
     "  -s, --size=SIZE            Accepted for compatibility (CPU sieve size).\n"
     "  -t, --threads=NUM          Accepted for compatibility (CPU threads).\n"
@@ -204,6 +217,26 @@ void help(int code) {
     "  -v, --version              Print version and license information."
     << std::endl;
   std::exit(code);
+}
+
+// primesieve N [START] --nth-prime (reference main.cpp:256-290)
+int nth_prime_mode(const Options& opts) {
+  if (opts.numbers.empty()) fail("missing n number");
+  const int64_t n = (int64_t) opts.numbers[0];
+  const uint64_t start = opts.numbers.size() > 1 ? opts.numbers[1] : 0;
+  primesieve::set_gpu_device(opts.gpu_device);
+  primesieve::set_gpu_enabled(true);
+  const std::string dev = primesieve::gpu_active_device();
+  if (dev.empty()) fail("could not initialise a GPU: " + primesieve::gpu_last_error());
+  if (!opts.quiet) std::cout << "GPU = " << dev << std::endl;
+  const auto t0 = std::chrono::steady_clock::now();
+  const uint64_t p = primesieve::nth_prime(n, start);
+  const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (opts.time)
+    std::cout << "Seconds: " << std::fixed << std::setprecision(3) << seconds << std::endl;
+  if (opts.quiet) std::cout << p << std::endl;
+  else std::cout << "Nth prime: " << p << std::endl;
+  return 0;
 }
 
 int run(int argc, char** argv) {
@@ -225,6 +258,7 @@ int run(int argc, char** argv) {
     for (const std::string& d : devices) std::cout << d << std::endl;
     return 0;
   }
+  if (opts.nth_prime) return nth_prime_mode(opts);
   if (opts.numbers.empty()) fail("missing STOP number");
   uint64_t start = 0, stop = opts.numbers[0];
   if (opts.numbers.size() >= 2) { start = opts.numbers[0]; stop = opts.numbers[1]; }
@@ -235,6 +269,19 @@ int run(int argc, char** argv) {
   const std::string dev = primesieve::gpu_active_device();
   if (dev.empty()) fail("could not initialise a GPU: " + primesieve::gpu_last_error());
   if (!opts.quiet) std::cout << "GPU = " << dev << std::endl;
+
+  if (opts.print) {                                       // primes, one per line
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<uint64_t> primes;
+    primesieve::generate_primes(start, stop, &primes);
+    const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::string buf;
+    for (uint64_t p : primes) { buf += std::to_string(p); buf += '\n'; }
+    std::cout << buf;
+    if (opts.time)
+      std::cout << "Seconds: " << std::fixed << std::setprecision(3) << seconds << std::endl;
+    return 0;
+  }
 
   const auto t0 = std::chrono::steady_clock::now();
   const std::array<uint64_t, 6> counts = primesieve::count_all(start, stop);

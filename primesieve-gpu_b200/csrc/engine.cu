@@ -909,6 +909,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
       a.num_bucket_lists = active_lists_;
     }
     const uint32_t g = (uint32_t) std::min<uint64_t>(grid_, ns);
+    a.bitmap_out = bitmap_out_ ? bitmap_out_ + (s0 - s_first) * seg_bytes_ : nullptr;
     timed_begin(0, st);
     cudaError_t e = launch_sieve(block_, all, g, smem_dyn_, st, a);
     timed_end(0, st);

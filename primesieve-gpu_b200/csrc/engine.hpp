@@ -113,6 +113,13 @@ public:
   // Estimated bucket storage of a planned range (bytes).
   size_t bucket_bytes(const RangePlan& p) const;
 
+  // Primes in [start, stop], ascending (sieve segments kept as bitmaps and
+  // turned into values on the device). Appended to out.
+  int generate_primes(uint64_t start, uint64_t stop, std::vector<uint64_t>& out, std::string& err);
+  // primesieve's nth_prime(n, start): n > 0 the nth prime > start, n = 0 as
+  // n = 1, n < 0 the |n|th prime < start.
+  int nth_prime(int64_t n, uint64_t start, uint64_t& prime, std::string& err);
+
   // Make sure the sieving-prime table covers sqrt(stop) (host work + upload).
   int prepare(uint64_t stop, std::string& err);
 
@@ -154,6 +161,9 @@ private:
   int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
+  // bitmap of [lo, hi] (lo >= 7) into host bytes, from segment base seg_low0
+  int sieve_bitmap(uint64_t lo, uint64_t hi, uint64_t& seg_low0, std::vector<uint8_t>& bits, std::string& err);
+  uint64_t count_range(uint64_t lo, uint64_t hi, std::string& err, int& rc);
   int count_enqueue(uint64_t start, uint64_t stop, uint32_t kinds,
                     unsigned long long* dev_counts, cudaStream_t st, std::string& err);
   void timed_begin(int which, cudaStream_t st);
@@ -213,6 +223,7 @@ private:
 
   unsigned long long* d_counts_ = nullptr;
   unsigned long long* h_counts_ = nullptr;   // pinned
+  uint8_t* bitmap_out_ = nullptr;            // set while run_windows stores bitmaps
 
   // batch storage
   unsigned long long* d_batch_rows_ = nullptr;

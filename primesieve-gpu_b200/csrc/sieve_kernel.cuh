@@ -67,6 +67,8 @@ struct SieveArgs {
   uint32_t wheel_tab[16];           // per class: bits, corr (wheel walk)
   uint32_t kinds;
   unsigned long long* counts;       // [6]
+  uint8_t* bitmap_out;              // optional: the sieved segments of this launch
+                                    // (edges masked), seg_bytes per segment
 };
 
 // x mod p for p < 2^32 with a precomputed rcp = floor((2^64-1)/p).
@@ -416,10 +418,12 @@ __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, ui
   }
 }
 
-// 5. mask the range edges [lo, hi] and count into acc.
+// 5. mask the range edges [lo, hi] and count into acc; with bm set, also
+// store the masked segment there (128-bit stores).
 template <int BLOCK, bool ALL_KINDS>
 __device__ __forceinline__ void phase_count(const uint4* smem4, uint32_t seg_bytes, uint64_t segLow,
-                                            uint64_t lo, uint64_t hi, uint32_t tid, uint64_t (&acc)[6]) {
+                                            uint64_t lo, uint64_t hi, uint32_t tid, uint64_t (&acc)[6],
+                                            uint4* bm = nullptr) {
   const uint32_t nchunks = seg_bytes >> 4;
   const uint64_t span = (uint64_t) seg_bytes * 30u;
   const uint64_t rhi = hi - segLow;                   // >= 7
@@ -442,6 +446,7 @@ __device__ __forceinline__ void phase_count(const uint4* smem4, uint32_t seg_byt
       }
       v = make_uint4(w4[0], w4[1], w4[2], w4[3]);
     }
+    if (bm) bm[ch] = v;
     count_word<ALL_KINDS>(v.x, c);
     count_word<ALL_KINDS>(v.y, c);
     count_word<ALL_KINDS>(v.z, c);
@@ -506,7 +511,8 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
     phase_direct<BLOCK>(a, a.n_primes, a.n_direct, sieve32, wheel_tab, segLow, tid);
     if (a.num_bucket_lists) phase_buckets(a, s, sieve32, &list_next, lane);
     __syncthreads();
-    phase_count<BLOCK, ALL_KINDS>(smem4, a.seg_bytes, segLow, a.lo, a.hi, tid, acc);
+    phase_count<BLOCK, ALL_KINDS>(smem4, a.seg_bytes, segLow, a.lo, a.hi, tid, acc,
+                                  a.bitmap_out ? reinterpret_cast<uint4*>(a.bitmap_out + s * a.seg_bytes) : nullptr);
     small_advance(sp, sr, sdl);
     __syncthreads();
   }

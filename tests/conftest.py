@@ -45,11 +45,24 @@ class Oracle:
         self.lib.oracle_count_wheel.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                                                 ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
         self.lib.oracle_ktuplet_table.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_uint8)]
+        self.lib.oracle_primes_u32.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                               ctypes.c_size_t]
+        self.lib.oracle_primes_u32.restype = ctypes.c_int64
 
     def plain(self, a, b, kinds=0x3F):
         out = (ctypes.c_uint64 * 6)()
         assert self.lib.oracle_count_plain(a, b, kinds, out) == 0
         return list(out)
+
+    def primes(self, lo, hi):
+        """The primes in [lo, hi], hi < 2^32."""
+        if hi < lo:
+            return []
+        cap = int((hi - lo) / 2) + 16
+        out = (ctypes.c_uint32 * cap)()
+        n = self.lib.oracle_primes_u32(lo, hi, out, cap)
+        assert n >= 0
+        return list(out[:n])
 
     def wheel(self, a, b, sieve_bytes=4096, kinds=0x3F):
         out = (ctypes.c_uint64 * 6)()

@@ -76,7 +76,9 @@ def test_cli_options_cpu(psg):
     assert r.returncode == 1 and "invalid option '-c7'" in r.stderr
     r = cli("2^64")
     assert r.returncode == 1 and "overflow" in r.stderr
-    r = cli("10", "--print")
+    r = cli("10", "--print=2")
+    assert r.returncode == 1 and "not supported" in r.stderr
+    r = cli("100", "--stress-test")
     assert r.returncode == 1 and "not supported" in r.stderr
     r = cli("--bogus")
     assert r.returncode == 1 and "unrecognized option" in r.stderr

@@ -102,3 +102,24 @@ def test_batch_fixture_pinned(oracle):
     short = sorted(rows, key=lambda r: r[1] - r[0])[:40]
     for a, b, k, want in short:
         assert oracle.plain(a, b, 1 << k)[k] == want, (a, b, k)
+
+
+def test_nth_prime_fixture_pinned(oracle):
+    """nth_prime.json (made by the reference library): every case whose
+    answer the plain oracle reaches quickly is a prime with exactly |n|
+    primes between start and it (n = 0 counts as 1)."""
+    import json
+    import os
+    from conftest import REPO
+    with open(os.path.join(REPO, "tests", "golden", "nth_prime.json")) as f:
+        data = json.load(f)
+    checked = 0
+    for n, start, p in data["nth"]:
+        k = max(1, abs(n))
+        lo, hi = (start + 1, p) if n >= 0 else (p, start - 1)
+        if hi - lo > 3 * 10 ** 7 or p > 10 ** 13:
+            continue
+        assert oracle.plain(p, p, 1)[0] == 1, (n, start, p)
+        assert oracle.plain(lo, hi, 1)[0] == k, (n, start, p)
+        checked += 1
+    assert checked >= 30
