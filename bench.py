@@ -377,6 +377,11 @@ def batch_section(psg, ctx, rank, world, args, torch, dist):
         return float(t.item())
 
     ctx.count_batch(q[:64])                      # warm-up
+    # per-class batch parameters, tuned on samples of these ranges (outside
+    # the timed region, like the sieving-prime table)
+    t = time.perf_counter()
+    tuned = ctx.autotune_batch(q, budget_seconds=25.0)
+    t_tune = time.perf_counter() - t
     ok = True
     times = []
     for _ in range(2):
@@ -410,6 +415,11 @@ def batch_section(psg, ctx, rank, world, args, torch, dist):
         "kernel_ms": {k: round(v[1], 2) for k, v in kst.items() if v[0]},
         "kernel_launches": {k: v[0] for k, v in kst.items() if v[0]},
         "api": "psg_count_batch vs psg_count per range (C ABI, host results)",
+        "autotune": {"seconds": round(t_tune, 2),
+                     "classes": [{"digits": r["range_class"] + 1, "direct_budget": r["direct_budget"],
+                                  "big_limit": r["big_limit"], "stripe": r["stripe"],
+                                  "sample_s": round(r["best_seconds"], 4), "default_s": round(r["default_seconds"], 4)}
+                                 for r in tuned]},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_batch_rate(rows, 10.0)

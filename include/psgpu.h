@@ -127,6 +127,27 @@ int psg_generate_primes(psg_context* ctx, uint64_t start, uint64_t stop,
  * messages. */
 int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime);
 
+/* Batch autotuner (no reference counterpart). Range classes are the decimal
+ * lengths of stop; for every class present in `ranges` a seeded sample of
+ * its ranges is counted under candidate parameters -- the batch-kernel vs
+ * bucket-path budget, the direct-tier extent of bucket-path ranges and the
+ * stripe length of work items -- and the fastest are kept in the context for
+ * psg_count_batch and the server. Stops after about budget_seconds. One
+ * report row per tuned class (up to cap rows; *count = rows). */
+typedef struct {
+  int32_t range_class;         /* decimal digits of stop - 1 */
+  uint32_t sample_ranges;
+  double sample_integers;
+  double direct_budget;        /* chosen: segments x primes past the shared state */
+  uint32_t big_limit;          /* chosen: direct tier below this prime (bucket-path ranges) */
+  uint32_t stripe;             /* chosen: segments per work item */
+  double best_seconds;         /* sample time with the chosen parameters */
+  double default_seconds;      /* sample time with the defaults */
+} psg_tune_class;
+
+int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, double budget_seconds,
+                       psg_tune_class* report, size_t cap, size_t* count);
+
 /* Build the sieving-prime table up to sqrt(stop) ahead of time. */
 int psg_prepare(psg_context* ctx, uint64_t stop);
 

@@ -30,6 +30,7 @@ PSG_SYMBOLS = (
     "psg_bucket_entries", "psg_measure_smem_atomic_rate", "psg_count_noalloc",
     "psg_server_start", "psg_server_submit", "psg_server_wait", "psg_server_replay",
     "psg_server_get_stats", "psg_server_stop", "psg_generate_primes", "psg_nth_prime",
+    "psg_autotune_batch",
 )
 
 
@@ -50,6 +51,13 @@ class PsgConfig(ctypes.Structure):
 class PsgRange(ctypes.Structure):
     _fields_ = [("start", ctypes.c_uint64), ("stop", ctypes.c_uint64),
                 ("kinds", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class PsgTuneClass(ctypes.Structure):
+    _fields_ = [("range_class", ctypes.c_int32), ("sample_ranges", ctypes.c_uint32),
+                ("sample_integers", ctypes.c_double), ("direct_budget", ctypes.c_double),
+                ("big_limit", ctypes.c_uint32), ("stripe", ctypes.c_uint32),
+                ("best_seconds", ctypes.c_double), ("default_seconds", ctypes.c_double)]
 
 
 class PsgServerConfig(ctypes.Structure):
@@ -110,6 +118,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_server_stop.restype = None
     lib.psg_generate_primes.argtypes = [vp, u64, u64, U64P, sz, ctypes.POINTER(sz)]
     lib.psg_nth_prime.argtypes = [vp, ctypes.c_int64, u64, U64P]
+    lib.psg_autotune_batch.argtypes = [vp, ctypes.POINTER(PsgRange), sz, ctypes.c_double,
+                                       ctypes.POINTER(PsgTuneClass), sz, ctypes.POINTER(sz)]
     for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
         fn = getattr(lib, "primesieve_count_" + name, None)
         if fn is not None:
@@ -215,6 +225,18 @@ class Context:
         p = ctypes.c_uint64(0)
         _check(self._lib.psg_nth_prime(self._h, n, start, ctypes.byref(p)))
         return p.value
+
+    def autotune_batch(self, ranges: Sequence[Tuple[int, int, int]], budget_seconds: float = 30.0) -> List[dict]:
+        """Tune the batch parameters per range class on samples of `ranges`."""
+        n = len(ranges)
+        arr = (PsgRange * max(n, 1))()
+        for i, (a, b, k) in enumerate(ranges):
+            arr[i].start, arr[i].stop, arr[i].kinds = a, b, k
+        cap = 32
+        rep = (PsgTuneClass * cap)()
+        cnt = ctypes.c_size_t(0)
+        _check(self._lib.psg_autotune_batch(self._h, arr, n, budget_seconds, rep, cap, ctypes.byref(cnt)))
+        return [{f: getattr(rep[i], f) for f, _ in PsgTuneClass._fields_} for i in range(min(cnt.value, cap))]
 
     def prepare(self, stop: int) -> None:
         _check(self._lib.psg_prepare(self._h, stop))

@@ -5,10 +5,10 @@
 //  * one sieving-prime table for the largest stop;
 //  * per range its prime tiers (small / medium with carried state / direct)
 //    and its class: a range whose primes beyond the shared state are few
-//    enough for its length (segments x such primes <= kDirectBudget) is
-//    sieved entirely by the persistent batch kernel; longer ranges with many
-//    big primes run through the windowed bucket path of run();
-//  * direct ranges are cut into stripes of <= kStripe segments (the medium
+//    enough for its length (segments x such primes <= the direct budget of
+//    its range class) is sieved entirely by the persistent batch kernel;
+//    longer ranges with many big primes run through the windowed bucket path;
+//  * direct ranges are cut into stripes of <= `stripe` segments (the medium
 //    state is set up once per stripe), ordered most expensive first, and
 //    served to the persistent grid from a device counter.
 // The ranges' rows are accumulated on the device and read back once.
@@ -17,6 +17,7 @@
 #include "../../include/psgpu.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -24,8 +25,6 @@ namespace psg {
 
 namespace {
 
-constexpr uint32_t kStripe = 8;            // segments per work item (at most)
-constexpr double kDirectBudget = 1e8;      // segments x direct primes per range
 
 #define PSG_CUDA(call)                                                          \
   do {                                                                          \
@@ -70,7 +69,7 @@ bool Engine::batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r
   const uint32_t n_small = std::min(n_small_all, n_total);
   const uint32_t n_med = std::max(n_small, std::min(n_total, n_small_all + state_cap_));
   const double direct = (double) (n_total - n_med);
-  if (direct > 0 && (direct * (double) nseg > kDirectBudget || nseg >= (1ull << 32))) return false;
+  if (direct > 0 && (direct * (double) nseg > batch_params(hi).direct_budget || nseg >= (1ull << 32))) return false;
   r.seg_low0 = seg_low0;
   r.lo = lo;
   r.hi = hi;
@@ -83,12 +82,13 @@ bool Engine::batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r
   return true;
 }
 
-// Stripes of <= kStripe segments of range `k` from segment s0 on, at most
+// Stripes of <= `stripe` segments (0: the range class's) of range `k` from segment s0 on, at most
 // max_seg segments in all; returns the segment after the last one taken.
 uint64_t Engine::append_stripes(uint32_t k, const BatchRange& r, double seg_cost, uint64_t s0, uint64_t max_seg,
-                                std::vector<BatchItem>& items, std::vector<double>& cost) const {
+                                std::vector<BatchItem>& items, std::vector<double>& cost, uint32_t stripe) const {
   const uint64_t nseg = range_segments(r);
-  const uint64_t nst = (nseg + kStripe - 1) / kStripe;
+  const uint32_t len_max = stripe ? stripe : batch_params(r.hi).stripe;
+  const uint64_t nst = (nseg + len_max - 1) / len_max;
   const uint64_t len = (nseg + nst - 1) / nst;
   uint64_t taken = 0;
   while (s0 < nseg && taken < max_seg) {
@@ -131,6 +131,93 @@ int Engine::launch_items(const BatchRange* d_ranges, const BatchItem* d_items, u
   cudaError_t e = launch_batch(b, st);
   timed_end(3, st);
   if (e != cudaSuccess) { err = std::string("batch kernel launch: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
+  return PSG_OK;
+}
+
+constexpr double kTuneSampleIntegers = 2e12;   // autotuner objective size per class
+constexpr double kTuneMargin = 0.03;           // a candidate must beat the defaults by this
+
+int Engine::batch_class(uint64_t stop) {
+  int d = 0;
+  for (uint64_t v = stop; v >= 10; v /= 10) d++;
+  return std::min(d, kBatchClasses - 1);
+}
+
+// Autotuner. Range class = decimal digits of stop. For every class present
+// in q: its ranges (all of them up to ~2e12 integers, else a selection by
+// length rank that keeps the longest) are counted once to warm up, then
+// timed under each candidate (direct budget x direct-tier extent); the class
+// keeps the fastest if it beats the defaults by more than 3%. (Small samples
+// under-fill the persistent grid and mislead the choice.)
+// Candidates are tried in order until budget_s is used up; the defaults
+// stay where nothing was timed.
+int Engine::autotune_batch(const RangeQuery* q, size_t n, double budget_s, std::vector<TuneReport>& report,
+                           std::string& err) {
+  using Clock = std::chrono::steady_clock;
+  const Clock::time_point t_start = Clock::now();
+  const auto elapsed = [&]() { return std::chrono::duration<double>(Clock::now() - t_start).count(); };
+  std::vector<std::vector<size_t>> by_class(kBatchClasses);
+  for (size_t i = 0; i < n; i++)
+    if (q[i].start <= q[i].stop && (q[i].kinds & 0x3fu) && q[i].stop >= 7)
+      by_class[batch_class(q[i].stop)].push_back(i);
+  const uint64_t span = (uint64_t) seg_bytes_ * 30u;
+  const uint32_t big_candidates[2] = { big_limit_, (uint32_t) std::min<uint64_t>(span / 4, 0xffffffffull) };
+  const double budgets[3] = { 1e7, 1e8, 1e9 };
+  const uint32_t stripes[1] = { 8 };
+  std::vector<uint64_t> rows;
+  int rc = PSG_OK;
+  for (int c = 0; c < kBatchClasses && elapsed() < budget_s; c++) {
+    std::vector<size_t>& idx = by_class[c];
+    if (idx.size() < 4) continue;
+    // objective: the class's own ranges (all of them up to ~kTuneSampleIntegers,
+    // else an evenly spaced selection by length rank that keeps the longest)
+    std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+      return q[x].stop - q[x].start > q[y].stop - q[y].start;
+    });
+    std::vector<RangeQuery> sample;
+    double ints = 0, total = 0;
+    for (size_t j : idx) total += (double) (q[j].stop - q[j].start) + 1.0;
+    const size_t stride = total <= kTuneSampleIntegers ? 1 : std::max<size_t>(1, (size_t) (total / kTuneSampleIntegers));
+    for (size_t j = 0; j < idx.size(); j += stride) {
+      sample.push_back(q[idx[j]]);
+      ints += (double) (q[idx[j]].stop - q[idx[j]].start) + 1.0;
+    }
+    rows.assign(6 * sample.size(), 0);
+    const BatchClassParams keep = batch_tune_[c];
+    TuneReport rep{};
+    rep.cls = c;
+    rep.sample_ranges = sample.size();
+    rep.sample_integers = ints;
+    rep.best_seconds = 1e30;
+    rep.default_seconds = 0;
+    BatchClassParams best = keep;
+    bool first = true;
+    for (double db : budgets)
+      for (uint32_t bl : big_candidates)
+        for (uint32_t st : stripes) {
+          if (!first && elapsed() > budget_s) break;
+          BatchClassParams cand;
+          cand.direct_budget = db;
+          cand.big_limit = bl;
+          cand.stripe = st;
+          batch_tune_[c] = cand;
+          if (first && (rc = count_batch(sample.data(), sample.size(), rows.data(), err))) return rc;   // warm-up
+          first = false;
+          const Clock::time_point t0 = Clock::now();
+          if ((rc = count_batch(sample.data(), sample.size(), rows.data(), err))) return rc;
+          const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
+          if (db == 1e8 && bl == big_limit_ && st == 8) rep.default_seconds = sec;
+          if (sec < rep.best_seconds) { rep.best_seconds = sec; best = cand; }
+        }
+    // keep the defaults unless a candidate wins clearly (timing noise)
+    if (rep.default_seconds > 0 && rep.best_seconds > (1.0 - kTuneMargin) * rep.default_seconds) {
+      best = keep;
+      rep.best_seconds = rep.default_seconds;
+    }
+    batch_tune_[c] = best;
+    rep.chosen = best;
+    report.push_back(rep);
+  }
   return PSG_OK;
 }
 
@@ -207,7 +294,10 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   }
   for (size_t j = 0; j < bucket_ranges.size(); j++) {
     const size_t i = bucket_ranges[j];
-    rc = run(lo[i], hi[i], kinds[i], d_batch_rows_ + 6 * (br.size() + j), stream_, err);
+    RangePlan p;
+    rc = plan_range(lo[i], hi[i], p, err, batch_params(hi[i]).big_limit);
+    if (rc) return rc;
+    rc = run_windows(p, kinds[i], d_batch_rows_ + 6 * (br.size() + j), stream_, 0, p.windows(), err);
     if (rc) return rc;
   }
 

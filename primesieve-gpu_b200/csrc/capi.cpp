@@ -266,6 +266,29 @@ int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime) 
   return rc ? fail(rc, err) : PSG_OK;
 }
 
+int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, double budget_seconds,
+                       psg_tune_class* report, size_t cap, size_t* count) {
+  if (!ctx || (n && !ranges) || (cap && !report)) return fail(PSG_ERR_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  std::string err;
+  std::vector<psg::TuneReport> rep;
+  int rc = ctx->engine.autotune_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, budget_seconds, rep, err);
+  if (rc) return fail(rc, err);
+  if (count) *count = rep.size();
+  for (size_t i = 0; i < rep.size() && i < cap; i++) {
+    psg_tune_class& o = report[i];
+    o.range_class = rep[i].cls;
+    o.sample_ranges = (uint32_t) rep[i].sample_ranges;
+    o.sample_integers = rep[i].sample_integers;
+    o.direct_budget = rep[i].chosen.direct_budget;
+    o.big_limit = rep[i].chosen.big_limit;
+    o.stripe = rep[i].chosen.stripe;
+    o.best_seconds = rep[i].best_seconds;
+    o.default_seconds = rep[i].default_seconds;
+  }
+  return PSG_OK;
+}
+
 int psg_prepare(psg_context* ctx, uint64_t stop) {
   if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
   std::lock_guard<std::mutex> lock(ctx->mu);

@@ -769,7 +769,8 @@ void Engine::fill_common_args(SieveArgs& a) const {
 }
 
 // Prime tiers and launch geometry of [lo, hi] (lo >= 7, lo <= hi).
-int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err) {
+int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit) {
+  const uint32_t big = big_limit ? big_limit : big_limit_;
   const uint64_t span = (uint64_t) seg_bytes_ * 30u;
   p.lo = lo;
   p.hi = hi;
@@ -784,10 +785,10 @@ int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err)
   p.n_total = upto(sq);
   p.n_small = std::min(below(small_limit_), p.n_total);
   // medium primes must fit the shared-memory state area
-  p.n_med = std::max(p.n_small, std::min({ below(big_limit_), p.n_total, p.n_small + state_cap_ }));
-  // beyond the shared state and below big_limit_: direct tier (no state);
+  p.n_med = std::max(p.n_small, std::min({ below(big), p.n_total, p.n_small + state_cap_ }));
+  // beyond the shared state and below big: direct tier (no state);
   // the rest go to buckets
-  p.n_dir = std::max(p.n_med, std::min(below(big_limit_), p.n_total));
+  p.n_dir = std::max(p.n_med, std::min(below(big), p.n_total));
   p.buckets = p.n_dir < p.n_total;
   // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
   p.n_sweep_end = std::max(p.n_dir, std::min(below(sweep_limit_), p.n_total));

@@ -44,6 +44,23 @@ uint32_t isqrt_u64(uint64_t x);
 // in the wheel-30 bit array): counts added to out[kind] when start <= 5.
 void small_table(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t out[6]);
 
+// Batch parameters of one range class (ranges whose stop has the same
+// number of decimal digits), set by Engine::autotune_batch.
+struct BatchClassParams {
+  double direct_budget = 1e8;   // segments x primes past the shared state: batch kernel up to this
+  uint32_t big_limit = 0;       // bucket-path ranges: direct tier below this prime (0: engine default)
+  uint32_t stripe = 8;          // segments per batch-kernel work item
+};
+constexpr int kBatchClasses = 21;   // stop < 10^20
+
+struct TuneReport {
+  int cls;                      // decimal digits of stop - 1
+  size_t sample_ranges;
+  double sample_integers;
+  BatchClassParams chosen;
+  double best_seconds, default_seconds;
+};
+
 // Prime tiers and launch geometry of one range [lo, hi] (lo >= 7):
 // primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
 // [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
@@ -92,7 +109,7 @@ public:
   // Tiers of [lo, hi] (lo >= 7) and launches of its windows [w0, w0 + nw);
   // counts added to dev_counts on st. The bucket storage is shared: windows
   // of different ranges must not overlap in time.
-  int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err);
+  int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit = 0);
   int run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
                   cudaStream_t st, uint64_t w0, uint64_t nw, std::string& err);
 
@@ -100,9 +117,15 @@ public:
   // tiers of [lo, hi] for the persistent kernel (false: needs the bucket
   // path), its stripes as work items, and one launch over device items.
   bool batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r, double& seg_cost);
+  // Per range class, time a sample of the batch's ranges of that class under
+  // candidate parameters and keep the fastest (wall-clock budget in seconds).
+  int autotune_batch(const RangeQuery* q, size_t n, double budget_s, std::vector<TuneReport>& report,
+                     std::string& err);
+  const BatchClassParams& batch_params(uint64_t stop) const { return batch_tune_[batch_class(stop)]; }
+  static int batch_class(uint64_t stop);
   uint64_t range_segments(const BatchRange& r) const;
   uint64_t append_stripes(uint32_t k, const BatchRange& r, double seg_cost, uint64_t s0, uint64_t max_seg,
-                          std::vector<BatchItem>& items, std::vector<double>& cost) const;
+                          std::vector<BatchItem>& items, std::vector<double>& cost, uint32_t stripe = 0) const;
   static void sort_items(std::vector<BatchItem>& items, const std::vector<double>& cost);
   int launch_items(const BatchRange* d_ranges, const BatchItem* d_items, uint32_t n_items,
                    unsigned long long* d_rows, uint32_t* d_queue, cudaStream_t st, std::string& err);
@@ -235,6 +258,7 @@ private:
   uint32_t* d_batch_queue_ = nullptr;
   std::vector<unsigned long long> h_batch_rows_;
   size_t batch_direct_ranges_ = 0, batch_bucket_ranges_ = 0, batch_items_ = 0;
+  BatchClassParams batch_tune_[kBatchClasses];
 
   // profiling
   bool profiling_ = false;

@@ -93,3 +93,15 @@ def test_batch_alone_equals_in_mix(ctx):
         assert alone[k] == want
         in_mix = ctx.count_batch(mix + [(a, b, 1 << k)] + mix[:50])[600]
         assert in_mix == alone
+
+
+def test_autotune_then_exact(psg):
+    """The autotuner changes only how ranges are scheduled: after tuning on a
+    sample every row of the fixture is still bit-exact."""
+    data = _load()
+    with psg.Context() as c:
+        rep = c.autotune_batch(_rows(data[:1500]), budget_seconds=20.0)
+        assert rep and all(r["best_seconds"] <= r["default_seconds"] + 1e-9 or r["default_seconds"] == 0 for r in rep)
+        got = c.count_batch(_rows(data))
+    bad = [(a, b, k, want, g) for (a, b, k, want), g in zip(data, got) if g[k] != want]
+    assert not bad, bad[:5]
