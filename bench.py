@@ -254,7 +254,10 @@ def main():
     ms_max = float(t.item())
     value = world * LENGTH * args.steps / (ms_max * 1e-3)
 
-    # ---- per-kernel roofline (CUDA events per launch, separate pass) --------
+    # ---- per-kernel roofline (CUDA events per launch, separate pass; the
+    # engine runs the windows of a profiled pass one after another, so each
+    # kernel's time is its own -- the timed passes overlap consecutive
+    # windows on two streams) ------------------------------------------------
     ctx.set_profiling(True)
     ctx.reset_kernel_stats()
     step()

@@ -194,8 +194,14 @@ Engine::~Engine() {
   cudaFree(d_pat_);
   cudaFree(d_primes_);
   cudaFree(d_recip_);
+  if (aux_stream_) cudaStreamSynchronize(aux_stream_);
   cudaFree(d_entries_);
   cudaFree(d_bcounts_);
+  cudaFree(d_entries2_);
+  cudaFree(d_bcounts2_);
+  if (fork_event_) cudaEventDestroy(fork_event_);
+  if (join_event_) cudaEventDestroy(join_event_);
+  if (aux_stream_) cudaStreamDestroy(aux_stream_);
   cudaFree(d_list_off_);
   cudaFree(d_list_cap_);
   cudaFree(d_chunk_begin_);
@@ -243,6 +249,9 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
     return PSG_ERR_NO_DEVICE;
   }
   PSG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  PSG_CUDA(cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking));
+  PSG_CUDA(cudaEventCreateWithFlags(&fork_event_, cudaEventDisableTiming));
+  PSG_CUDA(cudaEventCreateWithFlags(&join_event_, cudaEventDisableTiming));
   PSG_CUDA(cudaEventCreateWithFlags(&done_event_, cudaEventDisableTiming));
 
   // ---- geometry ------------------------------------------------------------
@@ -576,7 +585,7 @@ int Engine::prepare(uint64_t stop, std::string& err) {
 //    chunks cut for equal expected work (setup + hits per window).
 // Capacity = expected entries per segment + 6 sigma + 32 (x cap_scale_
 // after an overflow). All lists of one segment are packed in one region.
-int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::string& err) {
+int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStream_t st, std::string& err) {
   if (first == bucket_first_ && mid == bucket_mid_ && last == bucket_last_ && d_entries_) return PSG_OK;
   const double span = (double) seg_bytes_ * 30.0;
   const double per_seg = span * (8.0 / 30.0);
@@ -666,6 +675,21 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     PSG_CUDA(cudaMalloc(&d_bcounts_, need_counts * sizeof(uint32_t)));
     bcounts_cap_ = need_counts;
   }
+  // a second set of lists lets consecutive windows overlap on two streams;
+  // without the memory for it the windows run one after another
+  if (need_entries > entries2_cap_ || need_counts > bcounts2_cap_) {
+    cudaFree(d_entries2_); cudaFree(d_bcounts2_);
+    d_entries2_ = nullptr; d_bcounts2_ = nullptr; entries2_cap_ = bcounts2_cap_ = 0;
+    if (cudaMalloc(&d_entries2_, need_entries * sizeof(uint32_t)) == cudaSuccess &&
+        cudaMalloc(&d_bcounts2_, need_counts * sizeof(uint32_t)) == cudaSuccess) {
+      entries2_cap_ = need_entries;
+      bcounts2_cap_ = need_counts;
+    } else {
+      cudaGetLastError();
+      cudaFree(d_entries2_); cudaFree(d_bcounts2_);
+      d_entries2_ = nullptr; d_bcounts2_ = nullptr;
+    }
+  }
   if (lists + 1 > lists_cap_) {
     cudaFree(d_list_off_); cudaFree(d_list_cap_); cudaFree(d_chunk_begin_);
     PSG_CUDA(cudaMalloc(&d_list_off_, (lists + 1) * sizeof(uint32_t)));
@@ -679,12 +703,14 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     PSG_CUDA(cudaMalloc(&d_sweep_i_, (size_t) nsweep * sizeof(uint32_t)));
     sweep_state_cap_ = nsweep;
   }
-  PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
-  PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_));
+  PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   if (fill_ctas)
     PSG_CUDA(cudaMemcpyAsync(d_chunk_begin_, begin.data(), 2 * (fill_ctas + 1) * sizeof(uint32_t),
-                             cudaMemcpyHostToDevice, stream_));
-  PSG_CUDA(cudaStreamSynchronize(stream_));
+                             cudaMemcpyHostToDevice, st));
+  // the tables are uploaded on the launch stream, after every earlier window
+  // that reads them; the host vectors must outlive the copies
+  PSG_CUDA(cudaStreamSynchronize(st));
   seg_stride_ = stride;
   bucket_first_ = first;
   bucket_mid_ = mid;
@@ -814,7 +840,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   const bool use_buckets = p.buckets;
   int rc;
   if (use_buckets) {
-    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, err);
+    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, st, err);
     if (rc) return rc;
   }
 
@@ -830,9 +856,26 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
 
   const uint64_t s_first = w0 * step;
   const uint64_t s_last = std::min<uint64_t>(nseg, (w0 + nw) * step);
-  for (uint64_t s0 = s_first; s0 < s_last; s0 += step) {
+  // Two or more bucket windows: even windows on st with list set 0, odd ones
+  // on the auxiliary stream with set 1, so that the fill of one window can
+  // use the SMs the other window's kernels leave idle at their tails. The
+  // segment-major sweep carries state from window to window: no overlap.
+  // While profiling, windows run one after another so that each kernel's
+  // CUDA-event time is its own.
+  const bool two = use_buckets && !sweep_ctas_ && d_entries2_ && aux_stream_ && s_last - s_first > step &&
+                   !profiling_;
+  if (two) {
+    PSG_CUDA(cudaEventRecord(fork_event_, st));
+    PSG_CUDA(cudaStreamWaitEvent(aux_stream_, fork_event_, 0));
+  }
+  uint64_t k = 0;
+  for (uint64_t s0 = s_first; s0 < s_last; s0 += step, k++) {
     const uint64_t ns = std::min<uint64_t>(step, nseg - s0);
     const uint64_t win_low = seg_low0 + s0 * span;
+    const bool odd = two && (k & 1u);
+    cudaStream_t ws = odd ? aux_stream_ : st;
+    uint32_t* const w_entries = odd ? d_entries2_ : d_entries_;
+    uint32_t* const w_counts = odd ? d_bcounts2_ : d_bcounts_;
     a.seg_low0 = win_low;
     a.num_segments = ns;
     if (use_buckets) {
@@ -854,18 +897,18 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         w.list_off = d_list_off_;
         w.list_cap = d_list_cap_;
         w.seg_stride = seg_stride_;
-        w.entries = d_entries_;
-        w.counts = d_bcounts_;
+        w.entries = w_entries;
+        w.counts = w_counts;
         w.overflow = d_overflow_;
         w.entry_total = d_entry_total_;
         for (uint32_t c = 0; c < 8; c++) {
           w.wheel_tab[2 * c] = wheel_bits_packed(c);
           w.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
         }
-        timed_begin(2, st);
+        timed_begin(2, ws);
         bucket_sweep_kernel<32 * kSweepWarps, kSweepK>
-            <<<sweep_ctas_, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), st>>>(w);
-        timed_end(2, st);
+            <<<sweep_ctas_, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), ws>>>(w);
+        timed_end(2, ws);
         PSG_CUDA(cudaGetLastError());
       }
       if (fill_ctas_) {
@@ -891,33 +934,37 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.list_off = d_list_off_;
         b.list_cap = d_list_cap_;
         b.seg_stride = seg_stride_;
-        b.entries = d_entries_;
-        b.counts = d_bcounts_;
+        b.entries = w_entries;
+        b.counts = w_counts;
         b.overflow = d_overflow_;
         b.entry_total = d_entry_total_;
-        timed_begin(1, st);
+        timed_begin(1, ws);
         if (seg_pow2_)
-          bucket_fill_kernel<kBucketBlock, true><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), st>>>(b);
+          bucket_fill_kernel<kBucketBlock, true><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
         else
-          bucket_fill_kernel<kBucketBlock, false><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), st>>>(b);
-        timed_end(1, st);
+          bucket_fill_kernel<kBucketBlock, false><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
+        timed_end(1, ws);
         PSG_CUDA(cudaGetLastError());
       }
-      a.bucket_entries = d_entries_;
-      a.bucket_counts = d_bcounts_;
+      a.bucket_entries = w_entries;
+      a.bucket_counts = w_counts;
       a.bucket_list_off = d_list_off_;
       a.bucket_seg_stride = seg_stride_;
       a.num_bucket_lists = active_lists_;
     }
     const uint32_t g = (uint32_t) std::min<uint64_t>(grid_, ns);
     a.bitmap_out = bitmap_out_ ? bitmap_out_ + (s0 - s_first) * seg_bytes_ : nullptr;
-    timed_begin(0, st);
-    cudaError_t e = launch_sieve(block_, all, g, smem_dyn_, st, a);
-    timed_end(0, st);
+    timed_begin(0, ws);
+    cudaError_t e = launch_sieve(block_, all, g, smem_dyn_, ws, a);
+    timed_end(0, ws);
     if (e != cudaSuccess) {
       err = std::string("sieve kernel launch: ") + cudaGetErrorString(e);
       return PSG_ERR_CUDA;
     }
+  }
+  if (two) {
+    PSG_CUDA(cudaEventRecord(join_event_, aux_stream_));
+    PSG_CUDA(cudaStreamWaitEvent(st, join_event_, 0));
   }
   return PSG_OK;
 }

@@ -181,7 +181,7 @@ private:
   // big primes from this value on have at most ~8 multiples in a window of
   // w segments: the fill kernel walks them one lane per prime
   uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_; }
-  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
+  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, cudaStream_t st, std::string& err);
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
   // bitmap of [lo, hi] (lo >= 7) into host bytes, from segment base seg_low0
@@ -229,6 +229,11 @@ private:
   size_t entries_cap_ = 0;
   uint32_t* d_bcounts_ = nullptr;
   size_t bcounts_cap_ = 0;
+  uint32_t* d_entries2_ = nullptr;       // second list set (odd windows)
+  uint32_t* d_bcounts2_ = nullptr;
+  size_t entries2_cap_ = 0, bcounts2_cap_ = 0;
+  cudaStream_t aux_stream_ = nullptr;    // odd windows
+  cudaEvent_t fork_event_ = nullptr, join_event_ = nullptr;
   uint32_t* d_list_off_ = nullptr;
   uint32_t* d_list_cap_ = nullptr;
   uint32_t* d_chunk_begin_ = nullptr;
