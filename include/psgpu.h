@@ -192,8 +192,8 @@ int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
  * src/api.cpp:48-118). A worker thread owns the context's GPU and runs it in
  * steps: each step admits waiting requests into free device slots, runs one
  * launch of the persistent batch kernel over segment stripes taken
- * round-robin from the admitted requests plus one bucket window of the
- * oldest long high request, and completes the requests whose last piece ran.
+ * round-robin from the admitted requests plus up to two bucket windows of
+ * the oldest long high request, and completes the requests whose last piece ran.
  * Requests that arrive meanwhile join the next step. The sieving-prime table
  * stays resident (up to prime_limit, 2^32 by default: every 64-bit stop).
  * A request whose bucket storage would exceed the HBM budget is refused

@@ -759,7 +759,8 @@ void Engine::reset_kernel_stats() {
 }
 
 // Bucket storage the windows of p need: per segment, every list's expected
-// entries plus its margin (as ensure_buckets sizes them), times the window.
+// entries plus its margin (as ensure_buckets sizes them), times the window,
+// for both list sets (consecutive windows overlap).
 size_t Engine::bucket_bytes(const RangePlan& p) const {
   if (!p.buckets) return 0;
   const double per_seg = (double) seg_bytes_ * 30.0 * (8.0 / 30.0);
@@ -767,7 +768,7 @@ size_t Engine::bucket_bytes(const RangePlan& p) const {
   const double lists = std::max<double>(1.0, std::min<double>(lists_, p.n_total - p.n_dir));
   const double mu = total / lists;
   const double stride = lists * (mu + 6.0 * std::sqrt(mu) + 36.0) * cap_scale_;
-  return (size_t) (stride * (double) window_ * 4.0);
+  return (size_t) (2.0 * stride * (double) window_ * 4.0);
 }
 
 // Launch-wide sieve arguments: segment size, pre-sieve tables, sieving

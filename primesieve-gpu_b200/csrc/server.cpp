@@ -274,15 +274,18 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
     if (rc) return rc;
   }
 
-  // ---- one window of the oldest bucket-class request
+  // ---- one or two windows of the oldest bucket-class request
   Request* b = nullptr;
   for (Request* r : active_)
     if (r->bucket && r->next_win < r->nwin) { b = r; break; }
   if (b) {
     SRV_CUDA(cudaMemsetAsync(eng_.overflow_flag(), 0, sizeof(uint32_t), st_));
-    int rc = eng_.run_windows(b->plan, b->kinds, d_rows_ + 6ull * b->slot, st_, b->next_win, 1, err);
+    // two consecutive windows (they overlap on two streams) unless small
+    // requests are waiting: then short steps keep their latency down
+    const uint64_t nw = std::min<uint64_t>(items.empty() ? 2 : 1, b->nwin - b->next_win);
+    int rc = eng_.run_windows(b->plan, b->kinds, d_rows_ + 6ull * b->slot, st_, b->next_win, nw, err);
     if (rc) return rc;
-    b->next_win++;
+    b->next_win += nw;
     SRV_CUDA(cudaMemcpyAsync(h_flag_, eng_.overflow_flag(), sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
   }
 

@@ -7,8 +7,8 @@
 //      bucket storage would exceed the HBM budget is refused),
 //   2. takes segment stripes round-robin from the admitted batch-class
 //      requests (up to a segment budget) and runs them in one launch of the
-//      persistent batch kernel, and one window of the oldest bucket-class
-//      request on the windowed path,
+//      persistent batch kernel, and up to two windows of the oldest
+//      bucket-class request on the windowed path,
 //   3. reads back the rows of the requests whose last piece ran and
 //      completes them.
 // Requests that arrive while a step is on the GPU join the next step, so
