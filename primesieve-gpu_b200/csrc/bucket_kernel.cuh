@@ -220,6 +220,11 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
           put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ebit);
           // p >= win_bytes - b: no further hit (also keeps b + p from wrapping)
           b = (p >= win_bytes - b) ? kDone : b + p;
+          if (b != kDone) {                 // two multiples per step: half the loop overhead
+            const uint32_t sg2 = split_b(b, bo);
+            put(sg2, atomicAdd(&cnt[sg2], 1u), (bo << 3) | ebit);
+            b = (p >= win_bytes - b) ? kDone : b + p;
+          }
         }
       }
       const int more = __syncthreads_or(warp_done ? 0 : 1);

@@ -920,8 +920,9 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.seg_bytes = seg_bytes_;
         b.seg_magic = (uint32_t) ((1ull << 32) / seg_bytes_ + 1u);
         b.seg_shift = seg_shift_;
-        // steps per tile: a bin expects at most ~45% of its slots per tile
-        b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (0.45 * kBinCap * (double) ns / kBucketBlock));
+        // steps per tile (up to two entries per lane and step): a bin expects
+        // at most ~45% of its slots per tile
+        b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (0.225 * kBinCap * (double) ns / kBucketBlock));
         for (uint32_t c = 0; c < 8; c++) {
           b.wheel_tab[2 * c] = wheel_bits_packed(c);
           b.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
