@@ -35,6 +35,8 @@ struct BucketArgs {
   uint32_t seg_magic;         // floor(2^32 / seg_bytes) + 1 (segment index)
   uint32_t seg_shift;         // log2(seg_bytes) when it is a power of two
   uint32_t tile_steps;        // generate steps per warp between bin flushes
+  uint32_t flush_at;          // thread walk: entries in the bins that trigger a flush
+  uint32_t stagger_below;     // group walk: primes below this start staggered
   uint32_t wheel_tab[16];     // per class: bits, corr (wheel walk)
   const uint32_t* primes;
   const uint64_t* recip;
@@ -46,7 +48,8 @@ struct BucketArgs {
   const uint32_t* list_cap;   // [num_lists] capacity
   uint64_t seg_stride;        // entries per segment region
   uint32_t* entries;
-  uint32_t* counts;           // [win_segments][num_lists]
+  uint32_t* counts;           // [win_segments][num_lists] entries from the list's start
+  uint32_t* spill;            // [win_segments][num_lists] entries at the list's top (spills)
   uint32_t* overflow;         // set to 1 if any list overflowed
   unsigned long long* entry_total;  // running total of entries written
 };
@@ -68,11 +71,16 @@ __device__ __forceinline__ uint32_t seg_of(uint32_t b, uint32_t seg_bytes, uint3
 // in wheel class c -- one arithmetic progression of stride p bytes with a
 // fixed bit -- emitting one entry per step. An entry goes straight into its
 // segment's bin in shared memory (kBinCap slots per segment, rank from one
-// shared atomicAdd); an entry that finds its bin full is written to the HBM
-// list at once (rank from the CTA's per-segment HBM counter), so nothing is
-// ever dropped whatever the distribution. After tile_steps steps per warp the
-// CTA copies every bin to the end of its segment's HBM list, 8 lanes per bin,
-// as one contiguous run (HBM sees whole sectors, not scattered 4-byte writes).
+// shared atomicAdd); an entry that finds its bin full goes to its HBM list
+// at once, stored downward from the top of the list's capacity (rank from a
+// per-segment spill counter), so nothing is ever dropped whatever the
+// distribution and the list's main run stays whole quads. After tile_steps
+// steps per warp the CTA copies the whole quads of every bin to the end of
+// the main run with 16-byte stores, 4 lanes per bin; the 0-3 entries of a
+// bin's last partial quad move to the front of the bin and wait for the
+// next flush, and the CTA's final flush writes them as single entries. A
+// list is thus its main run [0, counts) followed, at [cap - spill, cap), by
+// its spills; the two overlap only if the list overflowed.
 // Primes with few multiples in a window (the CTA's thread_chunk range) are
 // walked one thread per prime through all 8 wheel classes (the medium tier's
 // wheel walk), so that locating a prime costs one lane, not eight; they
@@ -81,14 +89,16 @@ __device__ __forceinline__ uint32_t seg_of(uint32_t b, uint32_t seg_bytes, uint3
 // one rank atomic per segment run measured slower on B200: 42-47 ms against
 // 38 ms per pass on [1e15, 1e15+1e11].)
 constexpr uint32_t kBinCap = 32;          // bin slots per segment
-constexpr uint32_t kBinStride = 33;       // odd stride: bins start on different banks
+constexpr uint32_t kBinStride = 36;       // 16-byte rows; bins 4 apart start 16 banks apart
 
 // smem: thread-walk prime chunks rbuf[2][kChunk] (u64), pbuf[2][kChunk] |
-//       cnt[W] (entries of the tile per segment, may exceed kBinCap) |
-//       gcnt[W] (entries already in the HBM list) | bins[W][kBinStride]
+//       bins[W][kBinStride] (16-byte aligned) |
+//       cnt[W] (entries in the bin, plus spills since the last flush) |
+//       gcnt[W] (entries in the HBM list's main run, a multiple of 4 until
+//       the final flush) | gsp[W] (spilled entries at the list's top)
 constexpr uint32_t kChunk = 1024;         // thread-walk primes per chunk (= threads)
 constexpr size_t kChunkBytes = 2ull * kChunk * (8 + 4);
-constexpr size_t kFillBytesPerSegment = (2 + kBinStride) * 4;
+constexpr size_t kFillBytesPerSegment = (3 + kBinStride) * 4;
 constexpr size_t fill_smem_bytes(uint32_t W) {
   return kChunkBytes + (size_t) W * kFillBytesPerSegment;
 }
@@ -117,13 +127,14 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   const uint32_t W = a.win_segments;
   uint64_t* const rbuf = reinterpret_cast<uint64_t*>(smem_u32);  // [2][kChunk]
   uint32_t* const pbuf = smem_u32 + 4 * kChunk;  // [2][kChunk]
-  uint32_t* const cnt = pbuf + 2 * kChunk;       // [W]
+  uint32_t* const bins = pbuf + 2 * kChunk;      // [W][kBinStride], byte offset 24 KiB
+  uint32_t* const cnt = bins + W * kBinStride;   // [W]
   uint32_t* const gcnt = cnt + W;                // [W]
-  uint32_t* const bins = gcnt + W;               // [W][kBinStride]
+  uint32_t* const gsp = gcnt + W;                // [W]
   __shared__ uint32_t wheel_tab[16];
   __shared__ uint32_t s_total;                   // entries in the bins since the last flush
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-  for (uint32_t i = tid; i < 2 * W; i += BLOCK) cnt[i] = 0;
+  for (uint32_t i = tid; i < 3 * W; i += BLOCK) cnt[i] = 0;   // cnt, gcnt, gsp
   if (tid < 16) wheel_tab[tid] = a.wheel_tab[tid];
   if (tid == 0) s_total = 0;
   __syncthreads();
@@ -146,36 +157,59 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   const uint32_t g = lane >> 3;
   const uint32_t Q = cofactor_class(lane & 7u);
 
-  // emit one entry into its segment's bin (or straight into its HBM list)
+  // emit one entry into its segment's bin, or, the bin being full, straight
+  // into the top of its HBM list
   auto put = [&](uint32_t sg, uint32_t r, uint32_t e) {
     if (r < kBinCap) {
       bins[sg * kBinStride + r] = e;
     } else {
-      const uint32_t pos = atomicAdd(&gcnt[sg], 1u);
-      if (pos < cap) out[(uint64_t) sg * stride + pos] = e;
+      const uint32_t pos = atomicAdd(&gsp[sg], 1u);
+      if (pos < cap) out[(uint64_t) sg * stride + (cap - 1u - pos)] = e;
     }
   };
   auto split_b = [&](uint32_t b, uint32_t& bo) -> uint32_t {
     if (POW2) { bo = b & (seg_bytes - 1u); return b >> shift; }
     return seg_of(b, seg_bytes, magic, bo);
   };
-  // copy every bin to the end of its HBM list, 8 lanes per bin (all threads;
-  // the bins must be complete, i.e. after a barrier)
-  auto flush = [&]() {
-    const uint32_t q = lane >> 3, j = lane & 7u;
-    for (uint32_t s0 = warp * 4u; s0 < W; s0 += NWARPS * 4u) {   // warp-uniform trip count
-      const uint32_t sg = s0 + q;
+  // copy the whole quads of every bin to the end of its list's main run, 4
+  // lanes per bin and 8 bins per warp step (all threads; the bins must be
+  // complete, i.e. after a barrier). A bin's last partial quad moves to the
+  // bin's front, or, on the CTA's final flush, is written as single entries.
+  // The two bins of one 8-lane phase of a 128-bit shared load are 4 apart,
+  // 16 banks apart with the 36-word stride: conflict-free.
+  auto flush = [&](bool last) {
+    const uint32_t q = lane >> 2, j = lane & 3u;
+    const uint32_t slot = (q >> 1) + 4u * (q & 1u);
+    for (uint32_t s0 = warp * 8u; s0 < W; s0 += NWARPS * 8u) {   // warp-uniform trip count
+      const uint32_t sg = s0 + slot;
       const bool valid = sg < W;
-      const uint32_t c = valid ? cnt[sg] : 0u;
-      const uint32_t n = min(c, kBinCap);
-      const uint32_t base = valid ? gcnt[sg] : 0u;
+      const uint32_t n = valid ? min(cnt[sg], kBinCap) : 0u;
+      const uint32_t nq = n & ~3u;                   // entries in whole quads
+      const uint32_t base = valid ? gcnt[sg] : 0u;   // a multiple of 4
       const uint32_t room = base < cap ? cap - base : 0u;
-      const uint32_t nw = min(n, room);
-      const uint32_t* src = bins + sg * kBinStride;
+      const uint4* src = reinterpret_cast<const uint4*>(bins + sg * kBinStride);
       uint32_t* dst = out + (uint64_t) sg * stride + base;
-      for (uint32_t i = j; i < nw; i += 8u) dst[i] = src[i];
+      uint4 tail = make_uint4(0u, 0u, 0u, 0u);
+      for (uint32_t i = 4u * j; i < n; i += 16u) {
+        const uint4 v = src[i >> 2];
+        if (i + 4u > n) tail = v;                    // the partial quad
+        else if (i + 4u <= room) reinterpret_cast<uint4*>(dst)[i >> 2] = v;
+      }
       __syncwarp();
-      if (valid && j == 0) { gcnt[sg] = base + n; cnt[sg] = 0; }
+      const uint32_t rem = n & 3u;
+      if (rem && 4u * j == (nq & 15u)) {             // this lane read the partial quad
+        uint32_t* const t = last ? dst + nq : bins + sg * kBinStride;
+        const bool fits = !last || nq + rem <= room;
+        if (fits) {
+          t[0] = tail.x;
+          if (rem > 1u) t[1] = tail.y;
+          if (rem > 2u) t[2] = tail.z;
+        }
+      }
+      if (valid && j == 0) {
+        gcnt[sg] = base + (last ? n : nq);
+        cnt[sg] = last ? 0u : rem;
+      }
     }
     __syncthreads();
   };
@@ -183,6 +217,16 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   // ---- phase 1: group walk over primes [lo, hi), tiles of `steps` steps
   {
     uint32_t b = kDone, p = 0, ebit = 0;    // this lane's progression
+    uint32_t b0 = 0, bs = 0, end = 0;       // first multiple, start, current end (win_bytes, then bs)
+    const float stagger = (float) (warp * 4u + g) / (float) (NWARPS * 4u);   // one offset per prime group
+    // next multiple of the progression: up to the window's end, then from
+    // the first multiple up to the start (b + p < 2^32: p, b < win_bytes)
+    auto advance = [&](uint32_t x) -> uint32_t {
+      const uint32_t nx = x + p;
+      if (nx < end) return nx;
+      if (end == win_bytes && b0 < bs) { end = bs; return b0; }
+      return kDone;
+    };
     uint32_t group = warp;                  // next group of 4 primes of this warp
     bool warp_done = lo >= hi;
     uint32_t p_nx = 0;                      // prefetched prime of the next group
@@ -210,7 +254,23 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
             first_multiple(a.win_low, p, r_cur, d, c0);
             const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
             const uint64_t b64 = (d + (uint64_t) k * p) / 30u;   // byte index in window
-            if (b64 < win_bytes) b = (uint32_t) b64;
+            if (b64 < win_bytes) {
+              // primes with many multiples per window: start prime group
+              // G (of 4 * 32 per CTA) about G/128 of the way through the
+              // progression and wrap to its first multiple, so that the
+              // CTA's warps (all on similar primes) emit into different
+              // segments rather than together into the window's first ones
+              // and past their bins' capacity
+              b0 = (uint32_t) b64;
+              b = b0;
+              if (p < a.stagger_below) {
+                const uint32_t ks = (uint32_t) ((float) (win_bytes - b0) * __frcp_rz((float) p) * stagger);
+                const uint64_t bs64 = b64 + (uint64_t) ks * p;
+                if (bs64 < win_bytes) b = (uint32_t) bs64;
+              }
+              end = win_bytes;
+              bs = b;
+            }
             ebit = residue_to_bit((Q * (p % 30u)) % 30u);
           }
         }
@@ -218,17 +278,16 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
           uint32_t bo;
           const uint32_t sg = split_b(b, bo);
           put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ebit);
-          // p >= win_bytes - b: no further hit (also keeps b + p from wrapping)
-          b = (p >= win_bytes - b) ? kDone : b + p;
+          b = advance(b);
           if (b != kDone) {                 // two multiples per step: half the loop overhead
             const uint32_t sg2 = split_b(b, bo);
             put(sg2, atomicAdd(&cnt[sg2], 1u), (bo << 3) | ebit);
-            b = (p >= win_bytes - b) ? kDone : b + p;
+            b = advance(b);
           }
         }
       }
       const int more = __syncthreads_or(warp_done ? 0 : 1);
-      flush();
+      flush(!more && t_lo >= t_hi);     // the CTA's final flush writes the partial quads
       if (!more) break;
     }
   }
@@ -238,7 +297,7 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   // buffered), the bins are flushed when they may be getting full
   if (t_lo < t_hi) {
     const uint32_t nchunk = (t_hi - t_lo + kChunk - 1) / kChunk;
-    const uint32_t flush_at = (uint32_t) (0.45f * (float) kBinCap * (float) W);
+    const uint32_t flush_at = a.flush_at;
     auto issue = [&](uint32_t k) {
       const uint32_t i = t_lo + k * kChunk + tid;
       const bool in = i < t_hi;
@@ -282,7 +341,7 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
       __syncthreads();                            // chunk k consumed; s_total complete
       const bool full = s_total >= flush_at || k + 1 == nchunk;
       if (full) {
-        flush();
+        flush(k + 1 == nchunk);
         if (tid == 0) s_total = 0;
         __syncthreads();
       }
@@ -291,10 +350,15 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
 
   uint32_t written = 0;
   for (uint32_t sgi = tid; sgi < W; sgi += BLOCK) {
-    uint32_t c = gcnt[sgi];
-    if (c > cap) { atomicOr(a.overflow, 1u); c = cap; }
+    uint32_t c = gcnt[sgi], sp = gsp[sgi];
+    if ((uint64_t) c + sp > cap) {       // main run and spills met: recount
+      atomicOr(a.overflow, 1u);
+      c = min(c, cap);
+      sp = min(sp, cap - c);
+    }
     a.counts[(uint64_t) sgi * a.num_lists + list] = c;
-    written += c;
+    a.spill[(uint64_t) sgi * a.num_lists + list] = sp;
+    written += c + sp;
   }
   for (int o = 16; o > 0; o >>= 1) written += __shfl_xor_sync(0xffffffffu, written, o);
   if (lane == 0 && written) atomicAdd(a.entry_total, (unsigned long long) written);

@@ -38,6 +38,13 @@ namespace {
 constexpr int kBucketBlock = 1024;
 constexpr double kSetupGroup = 8.0;     // fill-chunk cost of locating a group-walk prime (entries)
 constexpr double kSetupThread = 4.0;    // ... of a thread-walk prime
+// Bucket fill bins: group-walk steps per warp between flushes (as a fill
+// fraction of the bins) and the thread walk's flush threshold; group-walk
+// primes with at least kStaggerMultiples multiples per class and window
+// start staggered by prime group.
+constexpr double kTileFill = 0.4;
+constexpr double kFlushFill = 0.6;
+constexpr uint64_t kStaggerMultiples = 16;
 constexpr int kSweepWarps = 16;     // sweep CTA = 512 threads
 constexpr int kSweepK = 16;         // sieving primes per sweep lane
 
@@ -669,7 +676,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStre
     }
     entries_cap_ = need_entries;
   }
-  const size_t need_counts = (size_t) lists * window_;
+  const size_t need_counts = 2 * (size_t) lists * window_;   // counts, then spill counts
   if (need_counts > bcounts_cap_) {
     cudaFree(d_bcounts_); d_bcounts_ = nullptr;
     PSG_CUDA(cudaMalloc(&d_bcounts_, need_counts * sizeof(uint32_t)));
@@ -922,7 +929,9 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.seg_shift = seg_shift_;
         // steps per tile (up to two entries per lane and step): a bin expects
         // at most ~45% of its slots per tile
-        b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (0.225 * kBinCap * (double) ns / kBucketBlock));
+        b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (kTileFill * kBinCap * (double) ns / kBucketBlock));
+        b.flush_at = (uint32_t) (kFlushFill * kBinCap * (double) ns);
+        b.stagger_below = (uint32_t) std::min<uint64_t>(((uint64_t) ns * seg_bytes_) / kStaggerMultiples, 0xffffffffull);
         for (uint32_t c = 0; c < 8; c++) {
           b.wheel_tab[2 * c] = wheel_bits_packed(c);
           b.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
@@ -938,6 +947,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.seg_stride = seg_stride_;
         b.entries = w_entries;
         b.counts = w_counts;
+        b.spill = w_counts + (size_t) active_lists_ * window_;
         b.overflow = d_overflow_;
         b.entry_total = d_entry_total_;
         timed_begin(1, ws);
@@ -950,7 +960,10 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
       }
       a.bucket_entries = w_entries;
       a.bucket_counts = w_counts;
+      a.bucket_spill = w_counts + (size_t) active_lists_ * window_;
+      a.bucket_spill_base = sweep_ctas_;
       a.bucket_list_off = d_list_off_;
+      a.bucket_list_cap = d_list_cap_;
       a.bucket_seg_stride = seg_stride_;
       a.num_bucket_lists = active_lists_;
     }

@@ -60,8 +60,12 @@ struct SieveArgs {
                               // first multiple recomputed every segment
   // big primes via buckets (num_bucket_lists == 0: none)
   const uint32_t* bucket_entries;   // [segment][seg_stride] entries
-  const uint32_t* bucket_counts;    // [segment][list] number of entries
+  const uint32_t* bucket_counts;    // [segment][list] entries from the list's start
+  const uint32_t* bucket_spill;     // [segment][list] entries at the list's top
+                                    // (lists >= bucket_spill_base only)
   const uint32_t* bucket_list_off;  // [list] offset inside a segment region
+  const uint32_t* bucket_list_cap;  // [list] capacity
+  uint32_t bucket_spill_base;       // first list with a spill region
   uint64_t bucket_seg_stride;       // entries per segment region
   uint32_t num_bucket_lists;        // lists per segment (0: no big primes)
   uint32_t wheel_tab[16];           // per class: bits, corr (wheel walk)
@@ -388,20 +392,26 @@ __device__ __forceinline__ void phase_direct(const SieveArgs& a, uint32_t first,
 
 // 4. big primes: the bucket lists of launch segment s. Warps take lists from
 // a shared counter (lists differ in length); each lane applies 4 entries per
-// 16-byte load (lists start 16-byte aligned). An entry is byte << 3 | bit
-// with byte < 2^20, so 0xffffffff never occurs and marks padding.
+// 16-byte load (lists start 16-byte aligned), then the list's spills, if
+// any, from the top of its capacity. An entry is byte << 3 | bit with
+// byte < 2^20, so 0xffffffff never occurs and marks padding.
 constexpr uint32_t kNoEntry = 0xffffffffu;   // padding past a list's end (never a real entry)
 __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, uint32_t* sieve32,
                                               uint32_t* list_next, uint32_t lane) {
   const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
+  const uint32_t* spill = a.bucket_spill + s * a.num_bucket_lists;
   const uint32_t* seg_entries = a.bucket_entries + s * a.bucket_seg_stride;
   for (;;) {
     uint32_t l = 0;
     if (lane == 0) l = atomicAdd(list_next, 1u);
     l = __shfl_sync(0xffffffffu, l, 0);
     if (l >= a.num_bucket_lists) break;
-    const uint32_t n = cnt[l];
-    const uint32_t* e = seg_entries + a.bucket_list_off[l];
+    // the list's length, spill count and place, loaded together
+    const bool has_spill = l >= a.bucket_spill_base;
+    const uint32_t n = __ldg(cnt + l);
+    const uint32_t ns = has_spill ? __ldg(spill + l) : 0u;
+    const uint32_t cap = has_spill ? __ldg(a.bucket_list_cap + l) : 0u;
+    const uint32_t* e = seg_entries + __ldg(a.bucket_list_off + l);
     const uint32_t n4 = n & ~3u;
     // four 16-byte loads in flight per lane before the atomics that use them
     // (one load per iteration left the warps waiting on HBM latency)
@@ -427,6 +437,14 @@ __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, ui
       const uint32_t v = __ldg(e + n4 + lane);
       const uint32_t bb = v >> 3;
       atomicAnd(&sieve32[bb >> 2], ~(1u << ((v & 7u) + 8u * (bb & 3u))));
+    }
+    if (ns) {
+      const uint32_t* top = e + cap - ns;
+      for (uint32_t x = lane; x < ns; x += 32u) {
+        const uint32_t v = __ldg(top + x);
+        const uint32_t bb = v >> 3;
+        atomicAnd(&sieve32[bb >> 2], ~(1u << ((v & 7u) + 8u * (bb & 3u))));
+      }
     }
   }
 }
