@@ -65,10 +65,10 @@ struct TuneReport {
 // primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
 // [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
 // n_sweep_end); sieve launches of `step` segments.
-// Medium (carried-state) primes below kMed8Limit -- at least 32 multiples
+// Medium (carried-state) primes below kMed8Limit -- at least 64 multiples
 // per 128 KiB segment -- are walked 8 lanes per prime, larger ones one
 // thread per prime.
-constexpr uint32_t kMed8Limit = 32768;
+constexpr uint32_t kMed8Limit = 16384;
 
 struct RangePlan {
   uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;

@@ -37,7 +37,7 @@ constexpr uint32_t kMaxPrimes = 23040;          // > pi(2^18) = 23000
 constexpr uint32_t kSegBytes = 131072;
 constexpr int kBlock = 1024;
 constexpr uint32_t kSmallLimit = 4096;
-constexpr uint32_t kMed8Limit = 32768;          // medium primes below: 8 lanes per prime
+constexpr uint32_t kMed8Limit = 16384;          // medium primes below: 8 lanes per prime
 
 // Scratch layout: [recip: u64 x kMaxPrimes][counts: u64 x 8][primes: u32 x kMaxPrimes]
 constexpr size_t kRecipOff = 0;
