@@ -287,6 +287,15 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   PSG_CUDA(cudaMemsetAsync(d_batch_rows_, 0, 6 * rows * sizeof(unsigned long long), stream_));
   PSG_CUDA(cudaMemsetAsync(d_overflow_, 0, sizeof(uint32_t), stream_));
 
+  // The bucket ranges' windows alternate between the two list sets across
+  // ranges (one range's fill overlaps the previous one's sieve), and the
+  // first ones may start on the auxiliary stream while the persistent kernel
+  // still drains: the chain starts after the row reset, before that launch.
+  struct Chain {
+    Engine* e; cudaStream_t st;
+    ~Chain() { e->chain_end(st); }
+  } chain{ this, stream_ };
+  if (!bucket_ranges.empty()) chain_begin(stream_);
   if (!items.empty()) {
     PSG_CUDA(cudaMemcpyAsync(d_batch_ranges_, br.data(), br.size() * sizeof(BatchRange), cudaMemcpyHostToDevice, stream_));
     PSG_CUDA(cudaMemcpyAsync(d_batch_items_, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, stream_));
@@ -302,6 +311,7 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
     rc = run_windows(p, kinds[i], d_batch_rows_ + 6 * (br.size() + j), stream_, 0, p.windows(), err);
     if (rc) return rc;
   }
+  chain_end(stream_);
 
   // ---- 5. results
   uint32_t overflow = 0;

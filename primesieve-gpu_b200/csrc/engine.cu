@@ -209,9 +209,12 @@ Engine::~Engine() {
   if (fork_event_) cudaEventDestroy(fork_event_);
   if (join_event_) cudaEventDestroy(join_event_);
   if (aux_stream_) cudaStreamDestroy(aux_stream_);
-  cudaFree(d_list_off_);
-  cudaFree(d_list_cap_);
-  cudaFree(d_chunk_begin_);
+  for (auto& sl : slots_) cudaFree(sl.d_table);
+  for (auto& g : stages_) {
+    if (g.ev) cudaEventSynchronize(g.ev);
+    if (g.h) cudaFreeHost(g.h);
+    if (g.ev) cudaEventDestroy(g.ev);
+  }
   cudaFree(d_sweep_b_);
   cudaFree(d_sweep_i_);
   cudaFree(d_overflow_);
@@ -592,8 +595,8 @@ int Engine::prepare(uint64_t stop, std::string& err) {
 //    chunks cut for equal expected work (setup + hits per window).
 // Capacity = expected entries per segment + 6 sigma + 32 (x cap_scale_
 // after an overflow). All lists of one segment are packed in one region.
-int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStream_t st, std::string& err) {
-  if (first == bucket_first_ && mid == bucket_mid_ && last == bucket_last_ && d_entries_) return PSG_OK;
+int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::string& err) {
+  if (plan_.last && first == plan_.first && mid == plan_.mid && last == plan_.last && d_entries_) return PSG_OK;
   const double span = (double) seg_bytes_ * 30.0;
   const double per_seg = span * (8.0 / 30.0);
   std::vector<uint32_t> off, cap, begin;
@@ -667,6 +670,11 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStre
   if (stride > 0xffffffffull) { err = "bucket region too large"; return PSG_ERR_LIMIT; }
 
   const size_t need_entries = (size_t) stride * window_;
+  const size_t need_counts = 2 * (size_t) lists * window_;   // counts, then spill counts
+  // buffers grow only when no window can still be using them
+  if (need_entries > entries_cap_ || need_counts > bcounts_cap_ || need_entries > entries2_cap_ ||
+      need_counts > bcounts2_cap_ || nsweep > sweep_state_cap_)
+    quiesce();
   if (need_entries > entries_cap_) {
     cudaFree(d_entries_); d_entries_ = nullptr; entries_cap_ = 0;
     if (cudaMalloc(&d_entries_, need_entries * sizeof(uint32_t)) != cudaSuccess) {
@@ -676,7 +684,6 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStre
     }
     entries_cap_ = need_entries;
   }
-  const size_t need_counts = 2 * (size_t) lists * window_;   // counts, then spill counts
   if (need_counts > bcounts_cap_) {
     cudaFree(d_bcounts_); d_bcounts_ = nullptr;
     PSG_CUDA(cudaMalloc(&d_bcounts_, need_counts * sizeof(uint32_t)));
@@ -697,35 +704,80 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, cudaStre
       d_entries2_ = nullptr; d_bcounts2_ = nullptr;
     }
   }
-  if (lists + 1 > lists_cap_) {
-    cudaFree(d_list_off_); cudaFree(d_list_cap_); cudaFree(d_chunk_begin_);
-    PSG_CUDA(cudaMalloc(&d_list_off_, (lists + 1) * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&d_list_cap_, (lists + 1) * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&d_chunk_begin_, 2 * (lists + 1) * sizeof(uint32_t)));
-    lists_cap_ = lists + 1;
-  }
   if (nsweep > sweep_state_cap_) {
     cudaFree(d_sweep_b_); cudaFree(d_sweep_i_);
     PSG_CUDA(cudaMalloc(&d_sweep_b_, (size_t) nsweep * sizeof(uint32_t)));
     PSG_CUDA(cudaMalloc(&d_sweep_i_, (size_t) nsweep * sizeof(uint32_t)));
     sweep_state_cap_ = nsweep;
   }
-  PSG_CUDA(cudaMemcpyAsync(d_list_off_, off.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  PSG_CUDA(cudaMemcpyAsync(d_list_cap_, cap.data(), lists * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  if (fill_ctas)
-    PSG_CUDA(cudaMemcpyAsync(d_chunk_begin_, begin.data(), 2 * (fill_ctas + 1) * sizeof(uint32_t),
-                             cudaMemcpyHostToDevice, st));
-  // the tables are uploaded on the launch stream, after every earlier window
-  // that reads them; the host vectors must outlive the copies
-  PSG_CUDA(cudaStreamSynchronize(st));
-  seg_stride_ = stride;
-  bucket_first_ = first;
-  bucket_mid_ = mid;
-  bucket_last_ = last;
-  active_lists_ = lists;
-  sweep_ctas_ = sweep_ctas;
-  fill_ctas_ = fill_ctas;
+  plan_.table.assign(off.begin(), off.end());
+  plan_.table.insert(plan_.table.end(), cap.begin(), cap.end());
+  if (fill_ctas) plan_.table.insert(plan_.table.end(), begin.begin(), begin.begin() + 2 * (fill_ctas + 1));
+  plan_.first = first;
+  plan_.mid = mid;
+  plan_.last = last;
+  plan_.geom.seg_stride = stride;
+  plan_.geom.lists = lists;
+  plan_.geom.sweep_ctas = sweep_ctas;
+  plan_.geom.fill_ctas = fill_ctas;
+  plan_.geom.first = first;
+  plan_.geom.mid = mid;
+  plan_gen_++;
   return PSG_OK;
+}
+
+// The current plan's tables for list set `set`, uploaded on ws (the stream
+// the set's windows run on, so after every earlier window that reads the
+// set's copy) unless the set holds them already. The upload source is a
+// pinned staging buffer that is reused only once its copy has run, so the
+// host never waits for the device here.
+int Engine::plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err) {
+  PlanSlot& sl = slots_[set];
+  if (sl.gen == plan_gen_) return PSG_OK;
+  const size_t n = plan_.table.size();
+  if (n > sl.cap) {
+    quiesce();                        // the old table may still be read
+    cudaFree(sl.d_table); sl.d_table = nullptr; sl.cap = 0;
+    PSG_CUDA(cudaMalloc(&sl.d_table, n * sizeof(uint32_t)));
+    sl.cap = n;
+  }
+  Stage& g = stages_[stage_next_];
+  stage_next_ = (stage_next_ + 1) % kStages;
+  if (g.used) PSG_CUDA(cudaEventSynchronize(g.ev));
+  if (n > g.cap) {
+    if (g.h) cudaFreeHost(g.h);
+    g.h = nullptr; g.cap = 0;
+    PSG_CUDA(cudaMallocHost(&g.h, n * sizeof(uint32_t)));
+    g.cap = n;
+  }
+  if (!g.ev) PSG_CUDA(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
+  std::memcpy(g.h, plan_.table.data(), n * sizeof(uint32_t));
+  PSG_CUDA(cudaMemcpyAsync(sl.d_table, g.h, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ws));
+  PSG_CUDA(cudaEventRecord(g.ev, ws));
+  g.used = true;
+  sl.gen = plan_gen_;
+  sl.geom = plan_.geom;
+  return PSG_OK;
+}
+
+// Wait for every window in flight (before bucket buffers are freed).
+void Engine::quiesce() {
+  cudaDeviceSynchronize();
+}
+
+void Engine::chain_begin(cudaStream_t st) {
+  if (!aux_stream_ || profiling_) return;
+  cudaEventRecord(fork_event_, st);
+  cudaStreamWaitEvent(aux_stream_, fork_event_, 0);
+  chain_ = true;
+  parity_ = 0;
+}
+
+void Engine::chain_end(cudaStream_t st) {
+  if (!chain_) return;
+  cudaEventRecord(join_event_, aux_stream_);
+  cudaStreamWaitEvent(st, join_event_, 0);
+  chain_ = false;
 }
 
 void Engine::timed_begin(int which, cudaStream_t st) {
@@ -849,7 +901,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   const bool use_buckets = p.buckets;
   int rc;
   if (use_buckets) {
-    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, st, err);
+    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, err);
     if (rc) return rc;
   }
 
@@ -866,30 +918,37 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
 
   const uint64_t s_first = w0 * step;
   const uint64_t s_last = std::min<uint64_t>(nseg, (w0 + nw) * step);
-  // Two or more bucket windows: even windows on st with list set 0, odd ones
-  // on the auxiliary stream with set 1, so that the fill of one window can
-  // use the SMs the other window's kernels leave idle at their tails. The
-  // segment-major sweep carries state from window to window: no overlap.
-  // While profiling, windows run one after another so that each kernel's
-  // CUDA-event time is its own.
-  const bool two = use_buckets && !sweep_ctas_ && d_entries2_ && aux_stream_ && s_last - s_first > step &&
-                   !profiling_;
-  if (two) {
+  // Two or more bucket windows (or any in a chain): alternate windows on st
+  // with list set 0 and on the auxiliary stream with set 1, so that the fill
+  // of one window can use the SMs the other window's kernels leave idle at
+  // their tails. The segment-major sweep carries state from window to
+  // window: no overlap. While profiling, windows run one after another so
+  // that each kernel's CUDA-event time is its own.
+  const bool two = use_buckets && !plan_.geom.sweep_ctas && d_entries2_ && aux_stream_ && !profiling_ &&
+                   (chain_ || s_last - s_first > step);
+  const bool fork = two && !chain_;
+  if (!chain_) parity_ = 0;
+  if (fork) {
     PSG_CUDA(cudaEventRecord(fork_event_, st));
     PSG_CUDA(cudaStreamWaitEvent(aux_stream_, fork_event_, 0));
   }
-  uint64_t k = 0;
-  for (uint64_t s0 = s_first; s0 < s_last; s0 += step, k++) {
+  for (uint64_t s0 = s_first; s0 < s_last; s0 += step) {
     const uint64_t ns = std::min<uint64_t>(step, nseg - s0);
     const uint64_t win_low = seg_low0 + s0 * span;
-    const bool odd = two && (k & 1u);
-    cudaStream_t ws = odd ? aux_stream_ : st;
-    uint32_t* const w_entries = odd ? d_entries2_ : d_entries_;
-    uint32_t* const w_counts = odd ? d_bcounts2_ : d_bcounts_;
+    const uint32_t set = two ? (parity_++ & 1u) : 0u;
+    cudaStream_t ws = set ? aux_stream_ : st;
+    uint32_t* const w_entries = set ? d_entries2_ : d_entries_;
+    uint32_t* const w_counts = set ? d_bcounts2_ : d_bcounts_;
     a.seg_low0 = win_low;
     a.num_segments = ns;
     if (use_buckets) {
-      if (sweep_ctas_) {
+      rc = plan_to_slot(set, ws, err);
+      if (rc) return rc;
+      const PlanGeom& gm = slots_[set].geom;
+      const uint32_t* const t_off = slots_[set].d_table;      // [lists] list offsets
+      const uint32_t* const t_cap = t_off + gm.lists;        // [lists] capacities
+      const uint32_t* const t_chunk = t_cap + gm.lists;      // fill chunk bounds
+      if (gm.sweep_ctas) {
         SweepArgs w;
         std::memset(&w, 0, sizeof w);
         w.win_low = win_low;
@@ -897,16 +956,16 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         w.seg_bytes = seg_bytes_;
         w.primes = d_primes_;
         w.recip = d_recip_;
-        w.first = bucket_first_;
-        w.n = bucket_mid_ - bucket_first_;
+        w.first = gm.first;
+        w.n = gm.mid - gm.first;
         w.init = (s0 == 0) ? 1u : 0u;
         w.state_b = d_sweep_b_;
         w.state_i = d_sweep_i_;
         w.list_base = 0;
-        w.num_lists_total = active_lists_;
-        w.list_off = d_list_off_;
-        w.list_cap = d_list_cap_;
-        w.seg_stride = seg_stride_;
+        w.num_lists_total = gm.lists;
+        w.list_off = t_off;
+        w.list_cap = t_cap;
+        w.seg_stride = gm.seg_stride;
         w.entries = w_entries;
         w.counts = w_counts;
         w.overflow = d_overflow_;
@@ -917,11 +976,11 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         }
         timed_begin(2, ws);
         bucket_sweep_kernel<32 * kSweepWarps, kSweepK>
-            <<<sweep_ctas_, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), ws>>>(w);
+            <<<gm.sweep_ctas, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), ws>>>(w);
         timed_end(2, ws);
         PSG_CUDA(cudaGetLastError());
       }
-      if (fill_ctas_) {
+      if (gm.fill_ctas) {
         BucketArgs b;
         std::memset(&b, 0, sizeof b);
         b.win_low = win_low;
@@ -940,34 +999,34 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         }
         b.primes = d_primes_;
         b.recip = d_recip_;
-        b.chunk_begin = d_chunk_begin_;
-        b.thread_chunk = d_chunk_begin_ + fill_ctas_ + 1;
-        b.list_base = sweep_ctas_;
-        b.num_lists = active_lists_;
-        b.list_off = d_list_off_;
-        b.list_cap = d_list_cap_;
-        b.seg_stride = seg_stride_;
+        b.chunk_begin = t_chunk;
+        b.thread_chunk = t_chunk + gm.fill_ctas + 1;
+        b.list_base = gm.sweep_ctas;
+        b.num_lists = gm.lists;
+        b.list_off = t_off;
+        b.list_cap = t_cap;
+        b.seg_stride = gm.seg_stride;
         b.entries = w_entries;
         b.counts = w_counts;
-        b.spill = w_counts + (size_t) active_lists_ * window_;
+        b.spill = w_counts + (size_t) gm.lists * window_;
         b.overflow = d_overflow_;
         b.entry_total = d_entry_total_;
         timed_begin(1, ws);
         if (seg_pow2_)
-          bucket_fill_kernel<kBucketBlock, true><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
+          bucket_fill_kernel<kBucketBlock, true><<<gm.fill_ctas, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
         else
-          bucket_fill_kernel<kBucketBlock, false><<<fill_ctas_, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
+          bucket_fill_kernel<kBucketBlock, false><<<gm.fill_ctas, kBucketBlock, fill_smem_bytes((uint32_t) ns), ws>>>(b);
         timed_end(1, ws);
         PSG_CUDA(cudaGetLastError());
       }
       a.bucket_entries = w_entries;
       a.bucket_counts = w_counts;
-      a.bucket_spill = w_counts + (size_t) active_lists_ * window_;
-      a.bucket_spill_base = sweep_ctas_;
-      a.bucket_list_off = d_list_off_;
-      a.bucket_list_cap = d_list_cap_;
-      a.bucket_seg_stride = seg_stride_;
-      a.num_bucket_lists = active_lists_;
+      a.bucket_spill = w_counts + (size_t) gm.lists * window_;
+      a.bucket_spill_base = gm.sweep_ctas;
+      a.bucket_list_off = t_off;
+      a.bucket_list_cap = t_cap;
+      a.bucket_seg_stride = gm.seg_stride;
+      a.num_bucket_lists = gm.lists;
     }
     const uint32_t g = (uint32_t) std::min<uint64_t>(grid_, ns);
     a.bitmap_out = bitmap_out_ ? bitmap_out_ + (s0 - s_first) * seg_bytes_ : nullptr;
@@ -979,7 +1038,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
       return PSG_ERR_CUDA;
     }
   }
-  if (two) {
+  if (fork) {
     PSG_CUDA(cudaEventRecord(join_event_, aux_stream_));
     PSG_CUDA(cudaStreamWaitEvent(st, join_event_, 0));
   }
@@ -1036,7 +1095,7 @@ int Engine::count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts
     // a bucket list overflowed: recount with larger lists
     overflow_retries_++;
     cap_scale_ *= 2.0;
-    bucket_first_ = bucket_mid_ = bucket_last_ = 0;
+    plan_.last = 0;
   }
   err = "bucket lists kept overflowing";
   return PSG_ERR_INTERNAL;

@@ -112,11 +112,17 @@ public:
   size_t batch_items() const { return batch_items_; }
 
   // Tiers of [lo, hi] (lo >= 7) and launches of its windows [w0, w0 + nw);
-  // counts added to dev_counts on st. The bucket storage is shared: windows
-  // of different ranges must not overlap in time.
+  // counts added to dev_counts on st. Bucket windows alternate between two
+  // list sets (set 0 on st, set 1 on the auxiliary stream), each with its
+  // own copy of the range's list tables; between chain_begin and chain_end
+  // the alternation continues from one call to the next, so that windows
+  // of consecutive ranges overlap too (the caller orders everything the
+  // ranges share before chain_begin and reads results after chain_end).
   int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit = 0);
   int run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
                   cudaStream_t st, uint64_t w0, uint64_t nw, std::string& err);
+  void chain_begin(cudaStream_t st);
+  void chain_end(cudaStream_t st);
 
   // Batch-kernel building blocks (also used by the request server):
   // tiers of [lo, hi] for the persistent kernel (false: needs the bucket
@@ -137,7 +143,7 @@ public:
   // Bucket-list overflow flag (device) and the response to it: lists grow
   // and the next windows are planned again.
   uint32_t* overflow_flag() { return d_overflow_; }
-  void grow_bucket_lists() { overflow_retries_++; cap_scale_ *= 2.0; bucket_first_ = bucket_mid_ = bucket_last_ = 0; }
+  void grow_bucket_lists() { overflow_retries_++; cap_scale_ *= 2.0; plan_.last = 0; }
   // Estimated bucket storage of a planned range (bytes).
   size_t bucket_bytes(const RangePlan& p) const;
 
@@ -186,7 +192,9 @@ private:
   // big primes from this value on have at most ~8 multiples in a window of
   // w segments: the fill kernel walks them one lane per prime
   uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_; }
-  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, cudaStream_t st, std::string& err);
+  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
+  int plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err);
+  void quiesce();
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
           cudaStream_t st, std::string& err);
   // bitmap of [lo, hi] (lo >= 7) into host bytes, from segment base seg_low0
@@ -239,13 +247,41 @@ private:
   size_t entries2_cap_ = 0, bcounts2_cap_ = 0;
   cudaStream_t aux_stream_ = nullptr;    // odd windows
   cudaEvent_t fork_event_ = nullptr, join_event_ = nullptr;
-  uint32_t* d_list_off_ = nullptr;
-  uint32_t* d_list_cap_ = nullptr;
-  uint32_t* d_chunk_begin_ = nullptr;
-  size_t lists_cap_ = 0;
-  uint64_t seg_stride_ = 0;
-  uint32_t bucket_first_ = 0, bucket_mid_ = 0, bucket_last_ = 0, active_lists_ = 0;
-  uint32_t sweep_ctas_ = 0, fill_ctas_ = 0, sweep_limit_ = 0;
+  // Bucket plan of the current big primes [first, last) (host): geometry and
+  // one u32 table [lists offsets | lists capacities | 2 (fill_ctas + 1)
+  // fill chunk bounds]; gen changes with every new plan.
+  struct PlanGeom {
+    uint64_t seg_stride = 0;              // entries per segment region
+    uint32_t lists = 0, sweep_ctas = 0, fill_ctas = 0, first = 0, mid = 0;
+  };
+  struct BucketPlan {
+    uint32_t first = 0, mid = 0, last = 0;   // last == 0: none
+    PlanGeom geom;
+    std::vector<uint32_t> table;
+  };
+  BucketPlan plan_;
+  uint64_t plan_gen_ = 0;
+  // device copy of a plan per list set, uploaded on the set's stream
+  struct PlanSlot {
+    uint64_t gen = 0;                      // plan_gen_ of the table it holds (0: none)
+    PlanGeom geom;
+    uint32_t* d_table = nullptr;
+    size_t cap = 0;
+  };
+  PlanSlot slots_[2];
+  // pinned upload sources, reused round robin once their copy has run
+  struct Stage {
+    uint32_t* h = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    bool used = false;
+  };
+  static constexpr int kStages = 8;
+  Stage stages_[kStages];
+  int stage_next_ = 0;
+  bool chain_ = false;                     // window sets alternate across run_windows calls
+  uint32_t parity_ = 0;                    // next window's list set (bit 0)
+  uint32_t sweep_limit_ = 0;
   uint32_t* d_sweep_b_ = nullptr;
   uint32_t* d_sweep_i_ = nullptr;
   size_t sweep_state_cap_ = 0;

@@ -130,6 +130,28 @@ def test_count_async_accumulates(ctx, psg):
     assert [x // 2 for x in dev.tolist()] == ctx.count(0, 10 ** 8)
 
 
+@pytest.mark.parametrize("a,b,k", [
+    (10 ** 15, 10 ** 15 + 10 ** 11, 1),            # bench workload: group-walk fill
+    (2 ** 64 - 2 ** 34, 2 ** 64 - 1, 63),          # thread-walk fill, all six kinds
+    (10 ** 18, 10 ** 18 + 10 ** 10, 1),
+    (10 ** 13, 10 ** 13 + 3 * 10 ** 10, 63),
+])
+def test_count_async_first_call_exact(psg, a, b, k):
+    """The asynchronous path has no overflow recount: on a fresh context (list
+    capacities at their defaults) its first count over bucket windows must
+    already be exact, i.e. no bucket list may overflow."""
+    import torch
+    with psg.Context() as c:
+        dev = torch.zeros(6, dtype=torch.int64, device="cuda")
+        c.count_async(a, b, k, dev.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        got = dev.tolist()
+        want = c.count(a, b, k)
+    assert got == want
+    if (a, k) == (10 ** 15, 1):
+        assert got[0] == 2895317534               # reference CPU library
+
+
 def test_c_api(psg, ctx):
     lib = psg.load()
     a, b = 10 ** 12, 10 ** 12 + 10 ** 8
