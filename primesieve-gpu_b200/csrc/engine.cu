@@ -735,11 +735,14 @@ int Engine::plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err) {
   PlanSlot& sl = slots_[set];
   if (sl.gen == plan_gen_) return PSG_OK;
   const size_t n = plan_.table.size();
+  // sized once for any plan of lists_ fill lists (no sweep lists): growing
+  // waits for every window in flight
+  const size_t want = std::max<size_t>(n, 4 * (size_t) lists_ + 8);
   if (n > sl.cap) {
-    quiesce();                        // the old table may still be read
+    if (sl.d_table) quiesce();        // the old table may still be read
     cudaFree(sl.d_table); sl.d_table = nullptr; sl.cap = 0;
-    PSG_CUDA(cudaMalloc(&sl.d_table, n * sizeof(uint32_t)));
-    sl.cap = n;
+    PSG_CUDA(cudaMalloc(&sl.d_table, want * sizeof(uint32_t)));
+    sl.cap = want;
   }
   Stage& g = stages_[stage_next_];
   stage_next_ = (stage_next_ + 1) % kStages;
@@ -747,8 +750,8 @@ int Engine::plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err) {
   if (n > g.cap) {
     if (g.h) cudaFreeHost(g.h);
     g.h = nullptr; g.cap = 0;
-    PSG_CUDA(cudaMallocHost(&g.h, n * sizeof(uint32_t)));
-    g.cap = n;
+    PSG_CUDA(cudaMallocHost(&g.h, want * sizeof(uint32_t)));
+    g.cap = want;
   }
   if (!g.ev) PSG_CUDA(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
   std::memcpy(g.h, plan_.table.data(), n * sizeof(uint32_t));
