@@ -132,11 +132,11 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   uint32_t* const gcnt = cnt + W;                // [W]
   uint32_t* const gsp = gcnt + W;                // [W]
   __shared__ uint32_t wheel_tab[16];
-  __shared__ uint32_t s_total;                   // entries in the bins since the last flush
+  __shared__ uint32_t s_round[3];                // thread walk: entries per round, 3 rotating slots
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   for (uint32_t i = tid; i < 3 * W; i += BLOCK) cnt[i] = 0;   // cnt, gcnt, gsp
   if (tid < 16) wheel_tab[tid] = a.wheel_tab[tid];
-  if (tid == 0) s_total = 0;
+  if (tid < 3) s_round[tid] = 0;
   __syncthreads();
 
   const uint32_t list = a.list_base + blockIdx.x;
@@ -298,6 +298,9 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   if (t_lo < t_hi) {
     const uint32_t nchunk = (t_hi - t_lo + kChunk - 1) / kChunk;
     const uint32_t flush_at = a.flush_at;
+    uint32_t rr = 0;                              // round slot (block-uniform)
+    uint32_t in_bins = 0;                         // entries since the last flush (block-uniform)
+    const float tstagger = (float) tid / (float) BLOCK;
     auto issue = [&](uint32_t k) {
       const uint32_t i = t_lo + k * kChunk + tid;
       const bool in = i < t_hi;
@@ -313,37 +316,86 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
       __syncthreads();                            // chunk k complete for every thread
       const uint32_t pc = pbuf[(k & 1u) * kChunk + tid];
       const uint64_t rc = rbuf[(k & 1u) * kChunk + tid];
+      // this thread's walk: byte tb of the next multiple and its wheel index
+      // j, running while tb < tend. A prime above half the window (at most
+      // two wheel rotations, 16 multiples) is walked at once; a smaller one
+      // starts about tid/1024 of the way through its rotations (p bytes
+      // each) and wraps to its first multiple (tb0, j0) once, in rounds:
+      // the CTA's threads then emit into different segments, not all into
+      // the window's first ones.
+      uint32_t tb = 0, tend = 0, tb0 = 0, tbs = 0, j = 0, j0 = 0, tpd = 0, tbits = 0, tcorr = 0;
+      const uint32_t two_p = pc < (1u << 30) ? 2u * pc : (1u << 31);   // round length, saturated
       uint32_t emitted = 0;
       if (pc != 0) {
         uint64_t d; uint32_t c0;
         first_multiple(a.win_low, pc, rc, d, c0);
-        uint32_t j = first_class_ge(c0);
+        j = first_class_ge(c0);
         const uint64_t b64 = (d + (uint64_t) (cofactor_class(j) - c0) * pc) / 30u;
         if (b64 < win_bytes) {
-          uint32_t tb = (uint32_t) b64;
-          const uint32_t tpd = pc / 30u;
+          tb = (uint32_t) b64;
+          tpd = pc / 30u;
           const uint32_t cls = residue_to_bit(pc - 30u * tpd);
-          const uint32_t tbits = wheel_tab[2 * cls], tcorr = wheel_tab[2 * cls + 1];
-          do {
-            uint32_t bo;
-            const uint32_t sg = split_b(tb, bo);
-            const uint32_t sh = 3u * j;
-            put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ((tbits >> sh) & 7u));
-            emitted++;
-            // tb < 2^31 and the step < 2^30: no wrap
-            tb += tpd * ((kGapPacked >> sh) & 7u) + ((tcorr >> sh) & 7u);
-            j = (j + 1u) & 7u;
-          } while (tb < win_bytes);
+          tbits = wheel_tab[2 * cls];
+          tcorr = wheel_tab[2 * cls + 1];
+          if (pc > (win_bytes >> 1)) {
+            do {
+              uint32_t bo;
+              const uint32_t sg = split_b(tb, bo);
+              const uint32_t sh = 3u * j;
+              put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ((tbits >> sh) & 7u));
+              emitted++;
+              // tb < 2^31 and the step < 2^30: no wrap
+              tb += tpd * ((kGapPacked >> sh) & 7u) + ((tcorr >> sh) & 7u);
+              j = (j + 1u) & 7u;
+            } while (tb < win_bytes);
+            tb = 0;                               // done (tend = 0)
+          } else {
+            tb0 = tb;
+            j0 = j;
+            const uint32_t q = (uint32_t) ((float) (win_bytes - tb0) * __frcp_rz((float) pc) * tstagger);
+            const uint64_t bs64 = b64 + (uint64_t) q * pc;        // q whole rotations on
+            if (bs64 < win_bytes) tb = (uint32_t) bs64;
+            tbs = tb;
+            tend = win_bytes;
+          }
         }
       }
-      emitted = __reduce_add_sync(kFull, emitted);
-      if (lane == 0 && emitted) atomicAdd(&s_total, emitted);
-      __syncthreads();                            // chunk k consumed; s_total complete
-      const bool full = s_total >= flush_at || k + 1 == nchunk;
-      if (full) {
-        flush(k + 1 == nchunk);
-        if (tid == 0) s_total = 0;
-        __syncthreads();
+      // rounds of at most 16 multiples per thread, so that the bins are
+      // flushed before they overflow however many multiples the primes have
+      for (;;) {
+        // a round ends after two wheel rotations (2p bytes, 16 multiples) or
+        // at the end of the run; the wrap to the first multiple happens
+        // between rounds
+        const uint32_t rend = (tb >= tend) ? tb : (tend - tb > two_p) ? tb + two_p : tend;
+        while (tb < rend) {
+          uint32_t bo;
+          const uint32_t sg = split_b(tb, bo);
+          const uint32_t sh = 3u * j;
+          put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ((tbits >> sh) & 7u));
+          emitted++;
+          // tb < 2^31 and the step < 2^30: no wrap
+          tb += tpd * ((kGapPacked >> sh) & 7u) + ((tcorr >> sh) & 7u);
+          j = (j + 1u) & 7u;
+        }
+        if (tb >= tend && tend == win_bytes && tb0 < tbs) { tb = tb0; j = j0; tend = tbs; }
+        // round rr adds to slot rr % 3 and clears slot (rr + 1) % 3, which no
+        // thread reads any more (its last reads were before the previous
+        // barrier) and none adds to before the next barrier: after this
+        // barrier every thread reads the same complete count, with no
+        // second barrier
+        emitted = __reduce_add_sync(kFull, emitted);
+        if (lane == 0 && emitted) atomicAdd(&s_round[rr], emitted);
+        if (tid == 0) s_round[rr == 2 ? 0 : rr + 1] = 0;
+        const int more = __syncthreads_or(tb < tend ? 1 : 0);
+        in_bins += s_round[rr];
+        rr = rr == 2 ? 0 : rr + 1;
+        const bool last = !more && k + 1 == nchunk;
+        if (in_bins >= flush_at || last) {
+          flush(last);                            // ends with a barrier
+          in_bins = 0;
+        }
+        if (!more) break;
+        emitted = 0;
       }
     }
   }

@@ -70,6 +70,10 @@ struct TuneReport {
 // thread per prime.
 constexpr uint32_t kMed8Limit = 16384;
 
+// Bucket fill: primes above the window's byte length / kThreadWalkDiv take
+// the thread walk, the rest the 8-lane group walk.
+constexpr uint32_t kThreadWalkDiv = 32;
+
 struct RangePlan {
   uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;
   uint32_t n_small = 0, n_med8 = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
@@ -189,9 +193,10 @@ private:
   double approx_prime(uint32_t i) const;
   double inv_prefix(uint32_t i) const;   // ~ sum of 1/p over table primes [0, i)
   uint32_t approx_count_below(uint64_t v) const;
-  // big primes from this value on have at most ~8 multiples in a window of
-  // w segments: the fill kernel walks them one lane per prime
-  uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_; }
+  // big primes from this value on have at most ~8 kThreadWalkDiv multiples
+  // in a window of w segments: the fill kernel walks them one lane per prime
+  // (one first-multiple setup instead of eight)
+  uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_ / kThreadWalkDiv; }
   int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
   int plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err);
   void quiesce();
