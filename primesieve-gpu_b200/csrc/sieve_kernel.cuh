@@ -441,9 +441,7 @@ __device__ __forceinline__ void phase_direct(const SieveArgs& a, uint32_t first,
 // 4. big primes: the bucket lists of launch segment s. Warps take lists from
 // a shared counter (lists differ in length); each lane applies 4 entries per
 // 16-byte load (lists start 16-byte aligned), then the list's spills, if
-// any, from the top of its capacity. An entry is byte << 3 | bit with
-// byte < 2^20, so 0xffffffff never occurs and marks padding.
-constexpr uint32_t kNoEntry = 0xffffffffu;   // padding past a list's end (never a real entry)
+// any, from the top of its capacity. An entry is byte << 3 | bit.
 __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, uint32_t* sieve32,
                                               uint32_t* list_next, uint32_t lane) {
   const uint32_t* cnt = a.bucket_counts + s * a.num_bucket_lists;
@@ -469,13 +467,13 @@ __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, ui
 #pragma unroll
       for (uint32_t u = 0; u < kBU; u++)
         v4[u] = (x0 + 128 * u < n4) ? __ldg(reinterpret_cast<const uint4*>(e + x0 + 128 * u))
-                                    : make_uint4(kNoEntry, kNoEntry, kNoEntry, kNoEntry);
+                                    : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
       for (uint32_t u = 0; u < kBU; u++) {
+        if (x0 + 128 * u >= n4) break;         // past the list's whole quads
         const uint32_t v[4] = { v4[u].x, v4[u].y, v4[u].z, v4[u].w };
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          if (v[q] == kNoEntry) continue;
           const uint32_t bb = v[q] >> 3;       // entry: byte index << 3 | bit
           atomicAnd(&sieve32[bb >> 2], ~(1u << ((v[q] & 7u) + 8u * (bb & 3u))));
         }
