@@ -75,8 +75,6 @@ bool Engine::batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r
   r.hi = hi;
   r.n_small = n_small;
   r.n_med_end = n_med;
-  r.n_med8 = std::min(std::max(n_small, count_primes_le(kMed8Limit, true)), n_med);
-  r.pad = 0;
   r.n_end = n_total;
   r.kinds = kinds;
   // sieve work + one reciprocal per direct prime

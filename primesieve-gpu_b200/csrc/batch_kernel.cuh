@@ -57,7 +57,6 @@ batch_sieve_kernel(const __grid_constant__ BatchArgs b)
     const BatchRange r = b.ranges[item.range];
     const uint64_t low0 = r.seg_low0 + (uint64_t) item.seg0 * span;
     const uint32_t n_med = r.n_med_end - r.n_small;
-    const uint32_t n_med8 = r.n_med8 - r.n_small;      // n_small <= n_med8 <= n_med_end
 
     small_setup<BLOCK>(a, r.n_small, low0 + 7, true, warp, lane, sp, sr, sdl);
     medium_setup<BLOCK>(a, r.n_small, n_med, mstate, low0, tid);
@@ -66,8 +65,7 @@ batch_sieve_kernel(const __grid_constant__ BatchArgs b)
       phase_presieve<BLOCK>(a, smem4, segLow, tid);
       __syncthreads();
       phase_small<BLOCK>(a, r.n_small, sieve32, segLow, warp, lane, sp, sr);
-      phase_medium8<BLOCK>(a, r.n_small, n_med8, mstate, sieve32, segLow, warp, lane);
-      phase_medium<BLOCK>(a, r.n_small + n_med8, n_med - n_med8, mstate + n_med8, sieve32, wheel_tab, segLow, tid);
+      phase_medium<BLOCK>(a, r.n_small, n_med, mstate, sieve32, wheel_tab, segLow, tid);
       phase_direct<BLOCK>(a, r.n_med_end, r.n_end, sieve32, wheel_tab, segLow, tid);
       __syncthreads();
       phase_count<BLOCK, true>(smem4, a.seg_bytes, segLow, r.lo, r.hi, tid, acc);

@@ -13,8 +13,6 @@ struct BatchRange {
   uint32_t n_med_end;           // primes[n_small, n_med_end): carried state
   uint32_t n_end;               // primes[n_med_end, n_end): direct
   uint32_t kinds;
-  uint32_t n_med8;              // primes[n_small, n_med8): 8 lanes per prime
-  uint32_t pad;
 };
 
 // A stripe of consecutive segments of one range.

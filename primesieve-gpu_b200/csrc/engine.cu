@@ -875,7 +875,6 @@ int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err,
   p.n_small = std::min(below(small_limit_), p.n_total);
   // medium primes must fit the shared-memory state area
   p.n_med = std::max(p.n_small, std::min({ below(big), p.n_total, p.n_small + state_cap_ }));
-  p.n_med8 = std::min(std::max(p.n_small, below(kMed8Limit)), p.n_med);
   // beyond the shared state and below big: direct tier (no state);
   // the rest go to buckets
   p.n_dir = std::max(p.n_med, std::min(below(big), p.n_total));
@@ -913,7 +912,6 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   a.lo = p.lo; a.hi = p.hi;
   a.n_small = p.n_small;
   a.n_primes = p.n_med;
-  a.n_med8 = p.n_med8;
   a.n_direct = p.n_dir;
   a.kinds = kinds;
   a.counts = dev_counts;

@@ -65,18 +65,13 @@ struct TuneReport {
 // primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
 // [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
 // n_sweep_end); sieve launches of `step` segments.
-// Medium (carried-state) primes below kMed8Limit -- at least 64 multiples
-// per 128 KiB segment -- are walked 8 lanes per prime, larger ones one
-// thread per prime.
-constexpr uint32_t kMed8Limit = 16384;
-
 // Bucket fill: primes above the window's byte length / kThreadWalkDiv take
 // the thread walk, the rest the 8-lane group walk.
 constexpr uint32_t kThreadWalkDiv = 32;
 
 struct RangePlan {
   uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;
-  uint32_t n_small = 0, n_med8 = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
+  uint32_t n_small = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
   bool buckets = false;
   uint64_t windows() const { return (nseg + step - 1) / step; }
 };

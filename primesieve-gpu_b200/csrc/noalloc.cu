@@ -37,7 +37,6 @@ constexpr uint32_t kMaxPrimes = 23040;          // > pi(2^18) = 23000
 constexpr uint32_t kSegBytes = 131072;
 constexpr int kBlock = 1024;
 constexpr uint32_t kSmallLimit = 4096;
-constexpr uint32_t kMed8Limit = 16384;          // medium primes below: 8 lanes per prime
 
 // Scratch layout: [recip: u64 x kMaxPrimes][counts: u64 x 8][primes: u32 x kMaxPrimes]
 constexpr size_t kRecipOff = 0;
@@ -193,7 +192,6 @@ extern "C" int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
     a.recip = reinterpret_cast<const uint64_t*>(d->scratch + kRecipOff);
     a.n_small = n_small;
     a.n_primes = n_total;
-    a.n_med8 = std::max(n_small, std::min<uint32_t>(n_total, (uint32_t) (std::lower_bound(g_host_primes, g_host_primes + g_host_nprimes, kMed8Limit) - g_host_primes)));
     for (uint32_t c = 0; c < 8; c++) {
       a.wheel_tab[2 * c] = psg::wheel_bits_packed(c);
       a.wheel_tab[2 * c + 1] = psg::wheel_corr_packed(c);

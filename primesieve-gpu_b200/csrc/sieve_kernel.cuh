@@ -54,10 +54,8 @@ struct SieveArgs {
   const uint32_t* primes;     // sieving primes (> presieve_max), ascending
   const uint64_t* recip;      // floor((2^64-1)/p) per prime
   uint32_t n_small;           // primes[0, n_small): warp-cooperative
-  uint32_t n_primes;          // primes[n_small, n_primes): carried state
-                              // (their state fits the shared-memory area);
-  uint32_t n_med8;            // of these, primes[n_small, n_med8): 8 lanes per
-                              // prime, the rest one thread per prime
+  uint32_t n_primes;          // primes[n_small, n_primes): thread per prime
+                              // (their state fits the shared-memory area)
   uint32_t n_direct;          // primes[n_primes, n_direct): thread per prime,
                               // first multiple recomputed every segment
   // big primes via buckets (num_bucket_lists == 0: none)
@@ -316,19 +314,44 @@ __device__ __forceinline__ void medium_setup(const SieveArgs& a, uint32_t first,
 }
 
 // One prime's sequential wheel walk from byte b (wheel index j) to the end
-// of the segment; returns the byte past the segment where it stopped.
+// of the segment; returns the byte past the segment where it stopped. Eight
+// consecutive multiples (one wheel rotation) span exactly p bytes and end
+// at the same wheel index, so while a whole rotation fits in the segment the
+// walk applies the 8 crossings at offsets and bits computed once, with no
+// per-step table lookups or bound checks; the rest goes step by step.
 __device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t* wheel_tab, uint32_t p,
                                                uint32_t b, uint32_t& j, uint32_t seg_bytes) {
   const uint32_t pdiv30 = p / 30u;
   const uint32_t cls = residue_to_bit(p - 30u * pdiv30);
   const uint32_t bits = wheel_tab[2 * cls];
   const uint32_t corr = wheel_tab[2 * cls + 1];
-  do {
+  if (p <= seg_bytes - b) {
+    uint32_t off[8];                 // off[0] = 0
+    uint32_t bitp = 0;               // bit of multiple k in bits 3k..3k+2
+    uint32_t o = 0, jj = j;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t sh = 3u * jj;
+      off[k] = o;
+      bitp |= ((bits >> sh) & 7u) << (3 * k);
+      o += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
+      jj = (jj + 1u) & 7u;
+    }
+    do {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t bk = b + off[k];
+        atomicAnd(&sieve32[bk >> 2], ~(1u << (((bitp >> (3 * k)) & 7u) + 8u * (bk & 3u))));
+      }
+      b += p;
+    } while (p <= seg_bytes - b);    // b <= seg_bytes here
+  }
+  while (b < seg_bytes) {
     const uint32_t sh = 3u * j;
     atomicAnd(&sieve32[b >> 2], ~(1u << (((bits >> sh) & 7u) + 8u * (b & 3u))));
     b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
     j = (j + 1u) & 7u;
-  } while (b < seg_bytes);
+  }
   return b;
 }
 
@@ -355,52 +378,6 @@ __device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first,
     }
     mstate[i] = st;
     p = pn;
-  }
-}
-
-// 3a. medium primes with many multiples per segment, primes[first, first+n):
-// 8 lanes per prime, lane c walking the multiples whose cofactor is in wheel
-// class c -- a stride-p progression with a fixed bit, one add per crossing
-// instead of the wheel walk's table step. Each lane derives its start from
-// the prime's carried state (byte b, class j of the next multiple v): the
-// next multiple of class c is v + p * ((Q_c - Q_j) mod 30), i.e. byte
-// b + ((v - x0) mod 30 + p * ((Q_c - Q_j) mod 30)) / 30, x0 = segLow + 7.
-// The new state is the smallest of the 8 lanes' first bytes past the
-// segment (a min over the 8-lane group), so the state is the same as the
-// wheel walk leaves it.
-template <int BLOCK>
-__device__ __forceinline__ void phase_medium8(const SieveArgs& a, uint32_t first, uint32_t n, uint32_t* mstate,
-                                              uint32_t* sieve32, uint64_t segLow, uint32_t warp, uint32_t lane) {
-  constexpr uint32_t NWARPS = BLOCK / 32;
-  const uint32_t seg_bytes = a.seg_bytes;
-  const uint32_t g = lane >> 3;                 // prime of the group of 4
-  const uint32_t c = lane & 7u;                 // wheel class of this lane
-  const uint32_t Qc = cofactor_class(c);
-  for (uint32_t i0 = warp * 4u; i0 < n; i0 += NWARPS * 4u) {   // warp-uniform trip count
-    const uint32_t i = i0 + g;
-    uint32_t key = kMedFar;
-    if (i < n) {
-      const uint32_t p = a.primes[first + i];
-      uint32_t st = mstate[i];
-      if (st == kMedFar) st = medium_state(segLow, p, a.recip[first + i]);
-      if (st != kMedFar) {
-        const uint32_t j = st & 7u;
-        const uint32_t pm = p % 30u;
-        const uint32_t Qj = cofactor_class(j);
-        const uint32_t dq = (Qc >= Qj) ? Qc - Qj : Qc + 30u - Qj;
-        const uint32_t rj = (pm * Qj + 23u) % 30u;            // (v - x0) mod 30
-        uint32_t b = (st >> 3) + (rj + p * dq) / 30u;         // p * dq < 2^32 (p < 2^27)
-        const uint32_t bit = residue_to_bit((pm * Qc) % 30u);
-        for (; b < seg_bytes; b += p)
-          atomicAnd(&sieve32[b >> 2], ~(1u << (bit + 8u * (b & 3u))));
-        const uint32_t nb = b - seg_bytes;
-        key = (nb < (1u << 29) - 1u) ? (nb << 3) | c : kMedFar;
-      }
-    }
-    key = min(key, __shfl_xor_sync(0xffffffffu, key, 1));
-    key = min(key, __shfl_xor_sync(0xffffffffu, key, 2));
-    key = min(key, __shfl_xor_sync(0xffffffffu, key, 4));
-    if (i < n && c == 0) mstate[i] = key;
   }
 }
 
@@ -562,7 +539,6 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
   const uint32_t warp = tid >> 5;
   const uint64_t span = (uint64_t) a.seg_bytes * 30u;
   const uint32_t n_med = a.n_primes - a.n_small;
-  const uint32_t n_med8 = (a.n_med8 > a.n_small) ? min(a.n_med8, a.n_primes) - a.n_small : 0u;
 
   // contiguous stripe of segments
   const uint64_t per = (a.num_segments + gridDim.x - 1) / gridDim.x;
@@ -585,8 +561,7 @@ sieve_count_kernel(const __grid_constant__ SieveArgs a)
     phase_presieve<BLOCK>(a, smem4, segLow, tid);
     __syncthreads();
     phase_small<BLOCK>(a, a.n_small, sieve32, segLow, warp, lane, sp, sr);
-    phase_medium8<BLOCK>(a, a.n_small, n_med8, mstate, sieve32, segLow, warp, lane);
-    phase_medium<BLOCK>(a, a.n_small + n_med8, n_med - n_med8, mstate + n_med8, sieve32, wheel_tab, segLow, tid);
+    phase_medium<BLOCK>(a, a.n_small, n_med, mstate, sieve32, wheel_tab, segLow, tid);
     phase_direct<BLOCK>(a, a.n_primes, a.n_direct, sieve32, wheel_tab, segLow, tid);
     if (a.num_bucket_lists) phase_buckets(a, s, sieve32, &list_next, lane);
     __syncthreads();
