@@ -68,6 +68,11 @@ CONFIGS = [
     dict(seg_bytes=4096, block=256, big_limit=300, sweep_limit=3000, window_segments=5),   # sweep + fill
     dict(seg_bytes=16384, block=512, big_limit=500, sweep_limit=500, bucket_lists=3),      # fill only
     dict(seg_bytes=32768, block=512, ctas_per_sm=2),
+    # segment size not a power of two: the fill's segment index by reciprocal
+    dict(seg_bytes=12288, block=256, big_limit=300, window_segments=9),
+    # thread walk with many wheel rotations per window: staggered starts,
+    # wraps, rounds and flushes between rounds
+    dict(seg_bytes=16384, block=1024, big_limit=2000, window_segments=64),
 ]
 
 
