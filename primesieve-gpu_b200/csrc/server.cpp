@@ -19,6 +19,11 @@ namespace {
   } while (0)
 
 constexpr uint32_t kDefaultSlots = 4096;
+// batch-kernel requests cost at most this many plain segments' work per
+// segment (~1.7 ms on one SM); costlier ones take the bucket path
+constexpr double kMaxSegCost = 16.0;
+// bucket windows per step: with batch-class work waiting, and without
+constexpr uint64_t kStepWindowsBusy = 2, kStepWindowsIdle = 4;
 
 } // namespace
 
@@ -213,7 +218,11 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
   // ---- plan the newly admitted requests
   for (Request* r : admitted) {
     const uint64_t lo = std::max<uint64_t>(r->start, 7), hi = r->stop;
-    if (eng_.batch_range(lo, hi, r->kinds, r->br, r->seg_cost)) {
+    // batch class unless the range needs the bucket path, or its segments
+    // are so costly (many direct-tier primes, each located again per
+    // segment on one SM) that the bucket path, which locates every prime
+    // once per window across all SMs, answers sooner
+    if (eng_.batch_range(lo, hi, r->kinds, r->br, r->seg_cost) && r->seg_cost <= kMaxSegCost) {
       r->bucket = false;
       r->nseg = eng_.range_segments(r->br);
       r->next_seg = 0;
@@ -261,6 +270,42 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
     }
   }
   Engine::sort_items(items, cost);
+
+  // ---- bucket-class windows: requests with the fewest windows left first
+  // (short requests do not queue behind long ones), the oldest request at
+  // least one window per step; their windows chain across requests, so one
+  // window's fill overlaps the previous one's sieve, and the chain starts
+  // before the persistent launch, so the first windows can take the SMs its
+  // tail leaves idle
+  std::vector<std::pair<Request*, uint64_t>> wplan;
+  {
+    std::vector<Request*> cand;
+    for (Request* r : active_)
+      if (r->bucket && r->next_win < r->nwin) cand.push_back(r);
+    if (!cand.empty()) {
+      Request* oldest = cand.front();
+      std::stable_sort(cand.begin(), cand.end(), [](const Request* x, const Request* y) {
+        return x->nwin - x->next_win < y->nwin - y->next_win;
+      });
+      uint64_t left = items.empty() ? kStepWindowsIdle : kStepWindowsBusy;
+      bool has_oldest = false;
+      for (Request* r : cand) {
+        if (left == 0) break;
+        const uint64_t nw = std::min<uint64_t>(left, r->nwin - r->next_win);
+        wplan.emplace_back(r, nw);
+        left -= nw;
+        has_oldest = has_oldest || r == oldest;
+      }
+      if (!has_oldest) wplan.emplace_back(oldest, 1);
+      SRV_CUDA(cudaMemsetAsync(eng_.overflow_flag(), 0, sizeof(uint32_t), st_));
+      eng_.chain_begin(st_);
+    }
+  }
+  struct Chain {
+    Engine& e; cudaStream_t st;
+    ~Chain() { e.chain_end(st); }
+  } chain{ eng_, st_ };
+
   if (!items.empty()) {
     if (items.size() > items_cap_) {
       cudaFree(d_items_);
@@ -274,32 +319,31 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
     if (rc) return rc;
   }
 
-  // ---- one or two windows of the oldest bucket-class request
-  Request* b = nullptr;
-  for (Request* r : active_)
-    if (r->bucket && r->next_win < r->nwin) { b = r; break; }
-  if (b) {
-    SRV_CUDA(cudaMemsetAsync(eng_.overflow_flag(), 0, sizeof(uint32_t), st_));
-    // two consecutive windows (they overlap on two streams) unless small
-    // requests are waiting: then short steps keep their latency down
-    const uint64_t nw = std::min<uint64_t>(items.empty() ? 2 : 1, b->nwin - b->next_win);
-    int rc = eng_.run_windows(b->plan, b->kinds, d_rows_ + 6ull * b->slot, st_, b->next_win, nw, err);
+  std::vector<Request*> ran;
+  for (auto& w : wplan) {
+    Request* r = w.first;
+    const int rc = eng_.run_windows(r->plan, r->kinds, d_rows_ + 6ull * r->slot, st_, r->next_win, w.second, err);
     if (rc) return rc;
-    b->next_win += nw;
-    SRV_CUDA(cudaMemcpyAsync(h_flag_, eng_.overflow_flag(), sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
+    r->next_win += w.second;
+    ran.push_back(r);
   }
+  eng_.chain_end(st_);
+  if (!wplan.empty())
+    SRV_CUDA(cudaMemcpyAsync(h_flag_, eng_.overflow_flag(), sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
 
   // ---- read back and complete
   int top = 0;
   for (Request* r : active_) top = std::max(top, r->slot + 1);
   SRV_CUDA(cudaMemcpyAsync(h_rows_, d_rows_, (size_t) top * 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st_));
   SRV_CUDA(cudaStreamSynchronize(st_));
-  if (b && *h_flag_) {
-    // a bucket list of this window overflowed: grow the lists and count the
-    // request again from its first window
+  if (!ran.empty() && *h_flag_) {
+    // a bucket list of one of this step's windows overflowed: grow the lists
+    // and count those requests again from their first windows
     eng_.grow_bucket_lists();
-    b->next_win = 0;
-    SRV_CUDA(cudaMemsetAsync(d_rows_ + 6ull * b->slot, 0, 6 * sizeof(unsigned long long), st_));
+    for (Request* r : ran) {
+      r->next_win = 0;
+      SRV_CUDA(cudaMemsetAsync(d_rows_ + 6ull * r->slot, 0, 6 * sizeof(unsigned long long), st_));
+    }
   }
   std::vector<Request*> still;
   for (Request* r : active_) {
