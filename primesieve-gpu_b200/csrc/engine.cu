@@ -117,9 +117,9 @@ __global__ void add_counts_kernel(unsigned long long* c, unsigned long long a0, 
 
 
 template <int BLOCK>
-void set_smem_attrs(uint32_t bytes) {
-  cudaFuncSetAttribute(sieve_count_kernel<BLOCK, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
-  cudaFuncSetAttribute(sieve_count_kernel<BLOCK, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
+void set_smem_attrs(int device) {
+  allow_max_dynamic_smem(sieve_count_kernel<BLOCK, false>, device);
+  allow_max_dynamic_smem(sieve_count_kernel<BLOCK, true>, device);
 }
 
 template <int BLOCK>
@@ -289,9 +289,9 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   state_cap_ = (budget - seg_bytes_) / 4u;
   smem_dyn_ = seg_bytes_ + 4u * state_cap_;
   switch (block_) {
-    case 256: set_smem_attrs<256>(smem_dyn_); break;
-    case 1024: set_smem_attrs<1024>(smem_dyn_); break;
-    default: set_smem_attrs<512>(smem_dyn_); break;
+    case 256: set_smem_attrs<256>(device_); break;
+    case 1024: set_smem_attrs<1024>(device_); break;
+    default: set_smem_attrs<512>(device_); break;
   }
   int occ = block_ == 256 ? occupancy<256>(smem_dyn_)
           : block_ == 1024 ? occupancy<1024>(smem_dyn_) : occupancy<512>(smem_dyn_);
@@ -317,13 +317,10 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   seg_pow2_ = (seg_bytes_ & (seg_bytes_ - 1u)) == 0;
   seg_shift_ = 0;
   while ((1u << seg_shift_) < seg_bytes_) seg_shift_++;
-  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) fill_smem_bytes(window_));
-  cudaFuncSetAttribute(bucket_fill_kernel<kBucketBlock, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) fill_smem_bytes(window_));
-  cudaFuncSetAttribute(primegen_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, 131072);
-  cudaFuncSetAttribute(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (window_ * sizeof(uint32_t)));
+  allow_max_dynamic_smem(bucket_fill_kernel<kBucketBlock, true>, device_);
+  allow_max_dynamic_smem(bucket_fill_kernel<kBucketBlock, false>, device_);
+  allow_max_dynamic_smem(primegen_kernel<1024>, device_);
+  allow_max_dynamic_smem(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>, device_);
   // sweep primes need pdiv30 < 2^22 (state packing): p < 1.25e8
   // (default: off -- the staged prime-major fill is faster on B200)
   sweep_limit_ = std::min<uint32_t>(cfg.sweep_limit, 120000000u);

@@ -121,9 +121,8 @@ int setup_device(int dev, DeviceSetup& d) {
   if (budget < kSegBytes) return fail(PSG_ERR_NO_DEVICE, "device has too little shared memory");
   d.state_cap = (budget - kSegBytes) / 4u;
   d.smem = kSegBytes + 4u * d.state_cap;
-  e = cudaFuncSetAttribute(psg::sieve_count_kernel<kBlock, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) d.smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(psg::sieve_count_kernel<kBlock, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) d.smem);
+  e = psg::allow_max_dynamic_smem(psg::sieve_count_kernel<kBlock, true>, dev);
+  if (e == cudaSuccess) e = psg::allow_max_dynamic_smem(psg::sieve_count_kernel<kBlock, false>, dev);
   if (e != cudaSuccess) return fail(PSG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   d.grid = (uint32_t) prop.multiProcessorCount;
   d.scratch = base;

@@ -35,6 +35,22 @@
 
 namespace psg {
 
+// The dynamic shared-memory limit of a kernel is one attribute for the whole
+// process, not per context: each context raises it to what the device allows
+// (less the kernel's static shared memory) instead of setting its own size,
+// so that a context with a smaller layout never lowers it under one with a
+// larger layout.
+template <typename Kernel>
+inline cudaError_t allow_max_dynamic_smem(Kernel kernel, int device) {
+  int optin = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int) fa.sharedSizeBytes);
+  return e;
+}
+
 constexpr int kMaxPresieveTables = 6;
 constexpr int kMaxPresievePrimes = 24;
 
@@ -361,12 +377,18 @@ __device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first,
                                              uint32_t* sieve32, const uint32_t* wheel_tab, uint64_t segLow,
                                              uint32_t tid) {
   const uint32_t seg_bytes = a.seg_bytes;
-  uint32_t i = tid;
-  uint32_t p = 0;
-  if (i < n) p = a.primes[first + i];
-  for (; i < n; i += BLOCK) {
-    const uint32_t inext = i + BLOCK;
+  // the primes of the next kMP iterations are loaded ahead (L2 latency)
+  constexpr uint32_t kMP = 2;
+  uint32_t pq[kMP];
+#pragma unroll
+  for (uint32_t u = 0; u < kMP; u++) pq[u] = (tid + u * BLOCK < n) ? a.primes[first + tid + u * BLOCK] : 0u;
+  for (uint32_t i = tid; i < n; i += BLOCK) {
+    const uint32_t inext = i + kMP * BLOCK;
     const uint32_t pn = (inext < n) ? a.primes[first + inext] : 0u;
+    const uint32_t p = pq[0];
+#pragma unroll
+    for (uint32_t u = 0; u + 1 < kMP; u++) pq[u] = pq[u + 1];
+    pq[kMP - 1] = pn;
     uint32_t st = mstate[i];
     if (st == kMedFar) st = medium_state(segLow, p, a.recip[first + i]);
     if (st != kMedFar) {
@@ -377,7 +399,6 @@ __device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first,
       st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kMedFar;
     }
     mstate[i] = st;
-    p = pn;
   }
 }
 

@@ -97,6 +97,19 @@ def test_engine_configs(psg, oracle, ref_counts, cfg):
         c.close()
 
 
+def test_contexts_with_different_layouts_coexist(psg, ctx):
+    """Kernel shared-memory limits are per process, not per context: a
+    context with small segments and windows, created and used after the
+    default one, must not shrink them under the default context's launches
+    (232 KB sieve, 204 KB bucket fill)."""
+    a, b = 10 ** 15, 10 ** 15 + 10 ** 10
+    before = ctx.count(a, b)
+    with psg.Context(seg_bytes=16384, block=1024, big_limit=2000, window_segments=3) as small:
+        assert small.count(10 ** 12, 10 ** 12 + 10 ** 8) == ctx.count(10 ** 12, 10 ** 12 + 10 ** 8)
+        assert ctx.count(a, b) == before
+        assert ctx.count_batch([(a, b, 63), (0, 10 ** 9, 63)]) == [before, ctx.count(0, 10 ** 9, 63)]
+
+
 def test_additivity_full_size(ctx, ref_counts, psg):
     """Size-independent property at the benchmark size: the six counts of
     [1e15, 1e15+1e11] equal the sum over 5 shards cut at == 2 (mod 30)."""
