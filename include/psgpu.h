@@ -103,7 +103,11 @@ int psg_count(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
 /* Asynchronous variant: ADDS the counts to dev_counts (device memory,
  * 6 x uint64_t) on `stream` (a cudaStream_t, NULL = the context's stream).
  * The 2/3/5 table is included. Host-side preparation (the sieving-prime
- * table for sqrt(stop)) happens before return. */
+ * table for sqrt(stop)) happens before return. Unlike psg_count it cannot
+ * recount when a bucket list overflows. The lists are sized for their
+ * expected length plus 6 sigma plus 32 entries, which no checked workload
+ * has exceeded; psg_count detects an overflow and recounts with larger
+ * lists. */
 int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
                     uint64_t* dev_counts, void* stream);
 

@@ -81,10 +81,11 @@ __device__ __forceinline__ uint32_t seg_of(uint32_t b, uint32_t seg_bytes, uint3
 // next flush, and the CTA's final flush writes them as single entries. A
 // list is thus its main run [0, counts) followed, at [cap - spill, cap), by
 // its spills; the two overlap only if the list overflowed.
-// Primes with few multiples in a window (the CTA's thread_chunk range) are
-// walked one thread per prime through all 8 wheel classes (the medium tier's
-// wheel walk), so that locating a prime costs one lane, not eight; they
-// stream through shared memory in chunks of one prime per thread.
+// Primes with at most ~32 multiples per class in a window (the CTA's
+// thread_chunk range, above the window's byte length / 32) are walked one
+// thread per prime through all 8 wheel classes (the medium tier's wheel
+// walk), so that locating a prime costs one lane, not eight; they stream
+// through shared memory in chunks of one prime per thread.
 // (A one-prime-per-warp walk emitting 32 consecutive multiples per step with
 // one rank atomic per segment run measured slower on B200: 42-47 ms against
 // 38 ms per pass on [1e15, 1e15+1e11].)
