@@ -61,14 +61,15 @@ struct TuneReport {
   double best_seconds, default_seconds;
 };
 
+// Bucket fill: primes above the window's byte length / kThreadWalkDiv take
+// the thread walk (one thread per prime), the rest the group walk (8 lanes
+// per prime, one per wheel class).
+constexpr uint32_t kThreadWalkDiv = 32;
+
 // Prime tiers and launch geometry of one range [lo, hi] (lo >= 7):
 // primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
 // [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
 // n_sweep_end); sieve launches of `step` segments.
-// Bucket fill: primes above the window's byte length / kThreadWalkDiv take
-// the thread walk, the rest the 8-lane group walk.
-constexpr uint32_t kThreadWalkDiv = 32;
-
 struct RangePlan {
   uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;
   uint32_t n_small = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
@@ -242,10 +243,10 @@ private:
   size_t entries_cap_ = 0;
   uint32_t* d_bcounts_ = nullptr;
   size_t bcounts_cap_ = 0;
-  uint32_t* d_entries2_ = nullptr;       // second list set (odd windows)
+  uint32_t* d_entries2_ = nullptr;       // second list set (windows on the auxiliary stream)
   uint32_t* d_bcounts2_ = nullptr;
   size_t entries2_cap_ = 0, bcounts2_cap_ = 0;
-  cudaStream_t aux_stream_ = nullptr;    // odd windows
+  cudaStream_t aux_stream_ = nullptr;    // windows of list set 1
   cudaEvent_t fork_event_ = nullptr, join_event_ = nullptr;
   // Bucket plan of the current big primes [first, last) (host): geometry and
   // one u32 table [lists offsets | lists capacities | 2 (fill_ctas + 1)
