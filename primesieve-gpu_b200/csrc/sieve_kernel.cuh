@@ -271,20 +271,22 @@ __device__ __forceinline__ void phase_small(const SieveArgs& a, uint32_t n_small
       const uint32_t rem = __shfl_sync(0xffffffffu, sr[m], l);
       const uint32_t pm = p % 30u;
       const uint64_t pp = (uint64_t) p * p;
-      uint64_t d; uint32_t c0;
-      if (x0 <= pp) {
-        d = pp - x0;
-        c0 = pm;
+      uint32_t b;
+      if (x0 <= pp) {                   // the segment starts before p^2
+        const uint64_t d = pp - x0;
         if (d >= span) continue;
-      } else {
+        const uint32_t k = (Q >= pm) ? Q - pm : Q + 30u - pm;
+        const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
+        if (b64 >= seg_bytes) continue;
+        b = (uint32_t) b64;
+      } else {                          // register-resident primes (the first 2048) are
+                                        // below 2^15: d + k p < 2^20, all in 32 bits
         const uint32_t dd = rem ? p - rem : 0u;
-        d = dd;
-        c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
+        const uint32_t c0 = (((7u + dd % 30u) % 30u) * inverse_mod30(pm)) % 30u;
+        const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
+        b = (dd + k * p) / 30u + r * p;
       }
-      const uint32_t k = (Q >= c0) ? Q - c0 : Q + 30u - c0;
-      const uint64_t b64 = (d + (uint64_t) k * p) / 30u + (uint64_t) r * p;
-      if (b64 < seg_bytes) {
-        const uint32_t b = (uint32_t) b64;
+      if (b < seg_bytes) {
         const uint32_t bit = residue_to_bit((Q * pm) % 30u);
         const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
         for (uint32_t w = b >> 2; w < nwords; w += p)
