@@ -335,8 +335,9 @@ __device__ __forceinline__ void medium_setup(const SieveArgs& a, uint32_t first,
 // of the segment; returns the byte past the segment where it stopped. Eight
 // consecutive multiples (one wheel rotation) span exactly p bytes and end
 // at the same wheel index, so while a whole rotation fits in the segment the
-// walk applies the 8 crossings at offsets and bits computed once, with no
-// per-step table lookups or bound checks; the rest goes step by step.
+// walk applies the 8 crossings at offsets computed once, with masks that only
+// rotate from one rotation to the next, and no per-step table lookups or
+// bound checks; the rest goes step by step.
 __device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t* wheel_tab, uint32_t p,
                                                uint32_t b, uint32_t& j, uint32_t seg_bytes) {
   const uint32_t pdiv30 = p / 30u;
@@ -355,11 +356,17 @@ __device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t
       o += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
       jj = (jj + 1u) & 7u;
     }
+    // the cleared bit of multiple k moves by 8 (p mod 4) bits (mod 32) from
+    // one rotation to the next: its inverted mask rotates
+    uint32_t m[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) m[k] = ~(1u << (((bitp >> (3 * k)) & 7u) + 8u * ((b + off[k]) & 3u)));
+    const uint32_t rot = 8u * (p & 3u);
     do {
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const uint32_t bk = b + off[k];
-        atomicAnd(&sieve32[bk >> 2], ~(1u << (((bitp >> (3 * k)) & 7u) + 8u * (bk & 3u))));
+        atomicAnd(&sieve32[(b + off[k]) >> 2], m[k]);
+        m[k] = __funnelshift_l(m[k], m[k], rot);
       }
       b += p;
     } while (p <= seg_bytes - b);    // b <= seg_bytes here
