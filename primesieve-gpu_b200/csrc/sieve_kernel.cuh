@@ -337,14 +337,18 @@ __device__ __forceinline__ void medium_setup(const SieveArgs& a, uint32_t first,
 // at the same wheel index, so while a whole rotation fits in the segment the
 // walk applies the 8 crossings at offsets computed once, with masks that only
 // rotate from one rotation to the next, and no per-step table lookups or
-// bound checks; the rest goes step by step.
+// bound checks. PARTIAL (medium primes, carried state): the last, partial
+// rotation uses the same offsets with a bound check each; otherwise (direct
+// primes, a few crossings per segment, for which the offsets do not pay) the
+// rest goes step by step.
+template <bool PARTIAL>
 __device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t* wheel_tab, uint32_t p,
                                                uint32_t b, uint32_t& j, uint32_t seg_bytes) {
   const uint32_t pdiv30 = p / 30u;
   const uint32_t cls = residue_to_bit(p - 30u * pdiv30);
   const uint32_t bits = wheel_tab[2 * cls];
   const uint32_t corr = wheel_tab[2 * cls + 1];
-  if (p <= seg_bytes - b) {
+  if (PARTIAL || p <= seg_bytes - b) {
     uint32_t off[8];                 // off[0] = 0
     uint32_t bitp = 0;               // bit of multiple k in bits 3k..3k+2
     uint32_t o = 0, jj = j;
@@ -362,20 +366,36 @@ __device__ __forceinline__ uint32_t wheel_walk(uint32_t* sieve32, const uint32_t
 #pragma unroll
     for (int k = 0; k < 8; k++) m[k] = ~(1u << (((bitp >> (3 * k)) & 7u) + 8u * ((b + off[k]) & 3u)));
     const uint32_t rot = 8u * (p & 3u);
-    do {
+    while (p <= seg_bytes - b) {     // b <= seg_bytes here
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         atomicAnd(&sieve32[(b + off[k]) >> 2], m[k]);
         m[k] = __funnelshift_l(m[k], m[k], rot);
       }
       b += p;
-    } while (p <= seg_bytes - b);    // b <= seg_bytes here
+    }
+    if constexpr (PARTIAL) {
+      // the crossings of the last, partial rotation; the first multiple past
+      // the segment is where the walk stops (the next rotation's first one,
+      // of the same wheel index, when all 8 fit)
+      uint32_t nb = b + p, jn = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t bk = b + off[k];
+        if (bk >= seg_bytes) { nb = bk; jn = (uint32_t) k; break; }
+        atomicAnd(&sieve32[bk >> 2], m[k]);
+      }
+      j = (j + jn) & 7u;
+      return nb;
+    }
   }
-  while (b < seg_bytes) {
-    const uint32_t sh = 3u * j;
-    atomicAnd(&sieve32[b >> 2], ~(1u << (((bits >> sh) & 7u) + 8u * (b & 3u))));
-    b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
-    j = (j + 1u) & 7u;
+  if constexpr (!PARTIAL) {
+    while (b < seg_bytes) {
+      const uint32_t sh = 3u * j;
+      atomicAnd(&sieve32[b >> 2], ~(1u << (((bits >> sh) & 7u) + 8u * (b & 3u))));
+      b += pdiv30 * ((kGapPacked >> sh) & 7u) + ((corr >> sh) & 7u);
+      j = (j + 1u) & 7u;
+    }
   }
   return b;
 }
@@ -403,7 +423,7 @@ __device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first,
     if (st != kMedFar) {
       uint32_t b = st >> 3;
       uint32_t j = st & 7u;
-      if (b < seg_bytes) b = wheel_walk(sieve32, wheel_tab, p, b, j, seg_bytes);
+      if (b < seg_bytes) b = wheel_walk<true>(sieve32, wheel_tab, p, b, j, seg_bytes);
       const uint32_t nb = b - seg_bytes;
       st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kMedFar;
     }
@@ -440,7 +460,7 @@ __device__ __forceinline__ void phase_direct(const SieveArgs& a, uint32_t first,
       uint32_t j = first_class_ge(c0);
       const uint32_t b = (uint32_t) ((d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u);
       if (b >= seg_bytes) continue;
-      wheel_walk(sieve32, wheel_tab, p, b, j, seg_bytes);
+      wheel_walk<false>(sieve32, wheel_tab, p, b, j, seg_bytes);
     }
   }
 }
