@@ -986,8 +986,10 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.seg_bytes = seg_bytes_;
         b.seg_magic = (uint32_t) ((1ull << 32) / seg_bytes_ + 1u);
         b.seg_shift = seg_shift_;
-        // steps per tile (up to two entries per lane and step): a bin expects
-        // at most ~45% of its slots per tile
+        // steps per tile (up to two entries per lane and step): with the
+        // staggered starts spreading a tile's entries over the window, a bin
+        // expects ~80% of its slots per tile (the overflow spills to the
+        // list's top); the thread walk flushes at 60%
         b.tile_steps = std::max<uint32_t>(1u, (uint32_t) (kTileFill * kBinCap * (double) ns / kBucketBlock));
         b.flush_at = (uint32_t) (kFlushFill * kBinCap * (double) ns);
         b.stagger_below = (uint32_t) std::min<uint64_t>(((uint64_t) ns * seg_bytes_) / kStaggerMultiples, 0xffffffffull);
