@@ -101,3 +101,36 @@ def test_split_range(psg, oracle):
         for x0, x1 in parts:
             total = [t + c for t, c in zip(total, oracle.plain(x0, x1))]
         assert total == oracle.plain(a, b)
+
+
+def test_shard_of_covers_range(psg):
+    """One process per GPU: the ranks' shards are disjoint, consecutive, cut
+    at == 2 (mod 30), and together cover [start, stop] exactly; ranks past
+    the last non-empty shard get None."""
+    import random
+    rnd = random.Random(3)
+    cases = [(0, 10, 4), (5, 5, 3), (0, 89, 8), (2 ** 64 - 1000, 2 ** 64 - 1, 5)]
+    cases += [(a, a + rnd.randrange(10 ** 7), rnd.randrange(1, 9)) for a in (rnd.randrange(10 ** 15) for _ in range(50))]
+    for a, b, world in cases:
+        shards = [psg.shard_of(a, b, r, world) for r in range(world)]
+        got = [s for s in shards if s is not None]
+        assert shards[:len(got)] == got                     # None only at the end
+        assert got[0][0] == a and got[-1][1] == b
+        for (x0, x1), (y0, y1) in zip(got, got[1:]):
+            assert x0 <= x1 and y0 == x1 + 1 and y0 % 30 == 2
+
+
+def test_serving_workload_stream(psg):
+    """The seed-1 serving stream is reproducible and has the stated shape:
+    Poisson arrivals at the rate, log-uniform starts and lengths, one kind per
+    request, stops clamped to 2^64 - 1."""
+    reqs, arr = psg.serving_workload(3000, 500.0)
+    assert (reqs, arr) == psg.serving_workload(3000, 500.0)
+    assert psg.serving_workload(50, 500.0, seed=2)[0] != reqs[:50]
+    assert all(t1 > t0 for t0, t1 in zip(arr, arr[1:]))
+    assert abs(arr[-1] / len(arr) - 1.0 / 500.0) < 0.1 / 500.0     # mean gap within 10%
+    for a, b, k in reqs:
+        assert 10 ** 6 <= a <= 1.8e19 and a <= b <= 2 ** 64 - 1
+        assert b - a + 1 <= 2 ** 36 and (b - a + 1 >= 2 ** 12 or b == 2 ** 64 - 1)
+        assert k in (1, 2, 4, 8, 16, 32)
+    assert len({k for _, _, k in reqs}) == 6
