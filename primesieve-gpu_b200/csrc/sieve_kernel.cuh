@@ -246,6 +246,29 @@ __device__ __forceinline__ void small_advance(uint32_t (&sp)[kSmallRegs], uint32
   }
 }
 
+// The progression w0, w0 + p, ... (< nwords) of one lane of a small prime.
+// The 32 lanes of a warp step by the same p words, so the bank pattern of
+// their first crossings repeats at every step; for primes below kSkewBelow
+// (over 64 steps per lane) each lane therefore starts delta = (lane - w0)
+// p^-1 (mod 32) steps in, where the word is == lane (mod 32) -- distinct
+// banks for all 32 lanes, step after step -- and crosses the skipped start
+// afterwards. (For larger primes the up to 31 extra steps of the warp's
+// longest lane cost more than the conflicts: 2048 -> 1024 -> 512 measured
+// 22.1 -> 21.4 -> 20.9 ms of sieve per pass on [1e15, 1e15+1e11].) p is odd,
+// so p^-1 mod 32 exists: p (2 - p p), one Newton step from p, the inverse
+// mod 8 of any odd p.
+constexpr uint32_t kSkewBelow = 512;
+__device__ __forceinline__ void small_walk(uint32_t* sieve32, uint32_t w0, uint32_t p, uint32_t nwords,
+                                           uint32_t mask, uint32_t lane) {
+  const uint32_t pinv = p * (2u - p * p);
+  const uint32_t ws = w0 + (((lane - w0) * pinv) & 31u) * p;
+  const uint32_t start = (p < kSkewBelow && ws < nwords) ? ws : w0;
+  for (uint32_t w = start; w < nwords; w += p)
+    atomicAnd(&sieve32[w], mask);
+  for (uint32_t w = w0; w < start; w += p)
+    atomicAnd(&sieve32[w], mask);
+}
+
 // 2. small primes: one warp per prime; lane (j = lane&7, r = lane>>3) walks
 // the multiples with cofactor class j, every 4th from phase r (stride p words).
 template <int BLOCK>
@@ -289,8 +312,7 @@ __device__ __forceinline__ void phase_small(const SieveArgs& a, uint32_t n_small
       if (b < seg_bytes) {
         const uint32_t bit = residue_to_bit((Q * pm) % 30u);
         const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
-        for (uint32_t w = b >> 2; w < nwords; w += p)
-          atomicAnd(&sieve32[w], mask);
+        small_walk(sieve32, b >> 2, p, nwords, mask, lane);
       }
     }
   }
@@ -307,8 +329,7 @@ __device__ __forceinline__ void phase_small(const SieveArgs& a, uint32_t n_small
       const uint32_t b = (uint32_t) b64;
       const uint32_t bit = residue_to_bit((Q * pm) % 30u);
       const uint32_t mask = ~(1u << (bit + 8u * (b & 3u)));
-      for (uint32_t w = b >> 2; w < nwords; w += p)
-        atomicAnd(&sieve32[w], mask);
+      small_walk(sieve32, b >> 2, p, nwords, mask, lane);
     }
   }
 }
