@@ -253,8 +253,9 @@ __device__ __forceinline__ void small_advance(uint32_t (&sp)[kSmallRegs], uint32
 // p^-1 (mod 32) steps in, where the word is == lane (mod 32) -- distinct
 // banks for all 32 lanes, step after step -- and crosses the skipped start
 // afterwards. (For larger primes the up to 31 extra steps of the warp's
-// longest lane cost more than the conflicts: 2048 -> 1024 -> 512 measured
-// 22.1 -> 21.4 -> 20.9 ms of sieve per pass on [1e15, 1e15+1e11].) p is odd,
+// longest lane cost more than the conflicts: skewing all small primes,
+// those below 1024 and those below 512 measured 22.1, 21.4 and 20.9 ms of
+// sieve per pass on [1e15, 1e15+1e11], 21.6 unskewed.) p is odd,
 // so p^-1 mod 32 exists: p (2 - p p), one Newton step from p, the inverse
 // mod 8 of any odd p.
 constexpr uint32_t kSkewBelow = 512;
