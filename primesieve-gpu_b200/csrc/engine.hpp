@@ -164,6 +164,8 @@ public:
   uint32_t seg_bytes() const { return seg_bytes_; }
   uint32_t block() const { return block_; }
   uint32_t grid() const { return grid_; }
+  // integers covered by one bucket window
+  uint64_t window_span() const { return (uint64_t) window_ * seg_bytes_ * 30u; }
   std::string describe() const;
 
   // Per-kernel CUDA-event timing (off by default).

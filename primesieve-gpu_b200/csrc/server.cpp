@@ -46,6 +46,20 @@ int Server::start(const ServerConfig& cfg, std::string& err) {
     size_t free_b = 0, total_b = 0;
     SRV_CUDA(cudaMemGetInfo(&free_b, &total_b));
     hbm_budget_ = cfg_.hbm_budget ? (size_t) cfg_.hbm_budget : (size_t) (0.8 * (double) free_b);
+    // warm-up: one full bucket window at the top of the table's reach (the
+    // largest bucket storage any request can need, so the lists never grow
+    // -- which waits for all work in flight -- while requests are served)
+    // and one small range through the persistent kernel, so that no
+    // request pays for buffer growth or a kernel's first launch
+    {
+      uint64_t c[6];
+      const uint64_t span = std::min<uint64_t>(eng_.window_span(), stop - 7);
+      rc = eng_.count(stop - span + 1, stop, 0x3f, c, err);
+      const RangeQuery q{ 1000000000ull, 1001000000ull, 0x3f, 0 };
+      uint64_t row[6];
+      if (rc == PSG_OK) rc = eng_.count_batch(&q, 1, row, err);
+      if (rc) return rc;
+    }
     const size_t slots = cfg_.max_slots;
     st_ = eng_.stream();
     SRV_CUDA(cudaMalloc(&d_ranges_, slots * sizeof(BatchRange)));
