@@ -341,18 +341,19 @@ cudaError_t Engine::launch_batch(const BatchArgs& b, cudaStream_t st) {
   static_assert(sizeof(BatchArgs) < 4000, "kernel parameter space");
   switch (block_) {
     case 256:
-      allow_max_dynamic_smem(batch_sieve_kernel<256>, device_);
+      if (!batch_smem_set_) allow_max_dynamic_smem(batch_sieve_kernel<256>, device_);
       batch_sieve_kernel<256><<<grid_, 256, smem_dyn_, st>>>(b);
       break;
     case 1024:
-      allow_max_dynamic_smem(batch_sieve_kernel<1024>, device_);
+      if (!batch_smem_set_) allow_max_dynamic_smem(batch_sieve_kernel<1024>, device_);
       batch_sieve_kernel<1024><<<grid_, 1024, smem_dyn_, st>>>(b);
       break;
     default:
-      allow_max_dynamic_smem(batch_sieve_kernel<512>, device_);
+      if (!batch_smem_set_) allow_max_dynamic_smem(batch_sieve_kernel<512>, device_);
       batch_sieve_kernel<512><<<grid_, 512, smem_dyn_, st>>>(b);
       break;
   }
+  batch_smem_set_ = true;                 // the limit only ever rises (see allow_max_dynamic_smem)
   return cudaGetLastError();
 }
 

@@ -283,6 +283,7 @@ private:
   Stage stages_[kStages];
   int stage_next_ = 0;
   bool chain_ = false;                     // window sets alternate across run_windows calls
+  bool batch_smem_set_ = false;            // persistent kernel's shared-memory limit raised
   uint32_t parity_ = 0;                    // next window's list set (bit 0)
   uint32_t sweep_limit_ = 0;
   uint32_t* d_sweep_b_ = nullptr;
