@@ -39,9 +39,9 @@ WORKLOAD = "count primes in [1e15, 1e15+1e11] (sieving primes <= 3.16e7, bucket 
 GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
 # ncu, [1e15, 1e15+2e9] (one window, 167,958,746 bucket entries):
 # fill kernel 612.604416 MB written + 67.080192 MB read, sieve kernel
-# 662.960384 MB read + 5.934592 MB written
+# 667.471872 MB read + 6.376192 MB written
 FILL_DRAM_BYTES_PER_ENTRY = (612.604416e6 + 67.080192e6) / 167958746
-SIEVE_DRAM_BYTES_PER_ENTRY = (662.960384e6 + 5.934592e6) / 167958746
+SIEVE_DRAM_BYTES_PER_ENTRY = (667.471872e6 + 6.376192e6) / 167958746
 
 
 def env_rank():
