@@ -445,7 +445,11 @@ __device__ __forceinline__ void phase_medium(const SieveArgs& a, uint32_t first,
     if (st != kMedFar) {
       uint32_t b = st >> 3;
       uint32_t j = st & 7u;
-      if (b < seg_bytes) b = wheel_walk<true>(sieve32, wheel_tab, p, b, j, seg_bytes);
+      // a prime above the segment length has under one rotation per
+      // segment: the offsets do not pay for it, the step walk is cheaper
+      if (b < seg_bytes)
+        b = (p <= seg_bytes) ? wheel_walk<true>(sieve32, wheel_tab, p, b, j, seg_bytes)
+                             : wheel_walk<false>(sieve32, wheel_tab, p, b, j, seg_bytes);
       const uint32_t nb = b - seg_bytes;
       st = (nb < (1u << 29) - 1u) ? (nb << 3) | j : kMedFar;
     }
