@@ -84,6 +84,14 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a few hundred ms to start: begin the timed region
+        # only once it has written its first sample (at most 5 s)
+        t = time.perf_counter()
+        while time.perf_counter() - t < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if not self.proc:
@@ -152,8 +160,9 @@ def reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    # per step: one bounded sample of the workload sized to ~6 s of CPU work
-    rate, n, el, kind, cores = cpu_reference_rate(6.0)
+    # per step: one bounded sample of the workload sized to ~6 s of CPU work,
+    # less when many steps are asked for (the whole run stays near 90 s)
+    rate, n, el, kind, cores = cpu_reference_rate(max(1.0, min(6.0, 90.0 / (args.warmup + args.steps))))
     exe = os.path.join(REPO, "oracle", "_ref", "primesieve")
     times = []
     for i in range(args.warmup + args.steps):
@@ -185,7 +194,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
