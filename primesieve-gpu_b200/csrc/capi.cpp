@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <cstddef>
+#include <exception>
 #include <mutex>
 #include <new>
 #include <string>
@@ -52,6 +53,22 @@ psg::EngineConfig to_engine(const psg_config* c) {
   return e;
 }
 
+// Runs the body of a C entry point; no C++ exception (a failed host
+// allocation, a thread that cannot start) may unwind through the C boundary,
+// each becomes a status and a message.
+template <typename F>
+int guarded(F&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(PSG_ERR_NOMEM, "out of host memory");
+  } catch (const std::exception& e) {
+    return fail(PSG_ERR_INTERNAL, std::string("internal error: ") + e.what());
+  } catch (...) {
+    return fail(PSG_ERR_INTERNAL, "internal error: unknown exception");
+  }
+}
+
 } // namespace
 
 namespace psg {
@@ -62,66 +79,79 @@ void set_last_error(const std::string& msg) { t_last_error = msg; }
 extern "C" {
 
 int psg_server_start(psg_context* ctx, const psg_server_config* cfg, psg_server** out) {
-  if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
-  *out = nullptr;
-  psg::ServerConfig c;
-  if (cfg) {
-    c.max_slots = cfg->max_slots;
-    c.step_segments = cfg->step_segments;
-    c.prime_limit = cfg->prime_limit;
-    c.hbm_budget = cfg->hbm_budget;
-  }
-  std::unique_ptr<psg_server> s(new (std::nothrow) psg_server{ std::make_unique<psg::Server>(ctx->engine, ctx->mu) });
-  if (!s) return fail(PSG_ERR_NOMEM, "out of host memory");
-  std::string err;
-  int rc = s->srv->start(c, err);
-  if (rc) return fail(rc, err);
-  *out = s.release();
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    psg::ServerConfig c;
+    if (cfg) {
+      c.max_slots = cfg->max_slots;
+      c.step_segments = cfg->step_segments;
+      c.prime_limit = cfg->prime_limit;
+      c.hbm_budget = cfg->hbm_budget;
+    }
+    std::unique_ptr<psg_server> s(new (std::nothrow) psg_server{ std::make_unique<psg::Server>(ctx->engine, ctx->mu) });
+    if (!s) return fail(PSG_ERR_NOMEM, "out of host memory");
+    std::string err;
+    int rc = s->srv->start(c, err);
+    if (rc) return fail(rc, err);
+    *out = s.release();
+    return PSG_OK;
+  });
 }
 
 int psg_server_submit(psg_server* s, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t* id) {
-  if (!s || !id) return fail(PSG_ERR_ARG, "NULL argument");
-  std::string err;
-  int rc = s->srv->submit(start, stop, kinds, *id, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!s || !id) return fail(PSG_ERR_ARG, "NULL argument");
+    std::string err;
+    int rc = s->srv->submit(start, stop, kinds, *id, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_server_wait(psg_server* s, uint64_t id, uint64_t counts[6], double* latency_seconds) {
-  if (!s) return fail(PSG_ERR_ARG, "NULL argument");
-  std::string err;
-  int rc = s->srv->wait(id, counts, latency_seconds, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!s) return fail(PSG_ERR_ARG, "NULL argument");
+    std::string err;
+    int rc = s->srv->wait(id, counts, latency_seconds, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_server_replay(psg_server* s, const psg_range* requests, const double* arrival_seconds,
                       size_t n, uint64_t* counts, double* latency_seconds) {
-  if (!s || (n && (!requests || !arrival_seconds))) return fail(PSG_ERR_ARG, "NULL argument");
-  for (size_t i = 1; i < n; i++)
-    if (arrival_seconds[i] < arrival_seconds[i - 1]) return fail(PSG_ERR_ARG, "arrival times must ascend");
-  std::string err;
-  int rc = s->srv->replay(reinterpret_cast<const psg::RangeQuery*>(requests), arrival_seconds, n, counts,
-                          latency_seconds, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!s || (n && (!requests || !arrival_seconds))) return fail(PSG_ERR_ARG, "NULL argument");
+    for (size_t i = 1; i < n; i++)
+      if (arrival_seconds[i] < arrival_seconds[i - 1]) return fail(PSG_ERR_ARG, "arrival times must ascend");
+    std::string err;
+    int rc = s->srv->replay(reinterpret_cast<const psg::RangeQuery*>(requests), arrival_seconds, n, counts,
+                            latency_seconds, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_server_get_stats(psg_server* s, psg_server_stats* out) {
-  if (!s || !out) return fail(PSG_ERR_ARG, "NULL argument");
-  const psg::ServerStats st = s->srv->stats();
-  out->submitted = st.submitted;
-  out->completed = st.completed;
-  out->refused = st.refused;
-  out->steps = st.steps;
-  out->bucket_requests = st.bucket_requests;
-  out->batch_requests = st.batch_requests;
-  out->integers = st.integers;
-  out->gpu_busy_seconds = st.gpu_busy_seconds;
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!s || !out) return fail(PSG_ERR_ARG, "NULL argument");
+    const psg::ServerStats st = s->srv->stats();
+    out->submitted = st.submitted;
+    out->completed = st.completed;
+    out->refused = st.refused;
+    out->steps = st.steps;
+    out->bucket_requests = st.bucket_requests;
+    out->batch_requests = st.batch_requests;
+    out->integers = st.integers;
+    out->gpu_busy_seconds = st.gpu_busy_seconds;
+    return PSG_OK;
+  });
 }
 
 void psg_server_stop(psg_server* s) {
   if (!s) return;
-  s->srv->stop();
+  try {
+    s->srv->stop();
+  } catch (...) {
+  }
   delete s;
 }
 
@@ -145,199 +175,233 @@ const char* psg_status_string(int s) {
 }
 
 int psg_device_count(int* count) {
-  if (!count) return fail(PSG_ERR_ARG, "count is NULL");
-  int n = 0;
-  cudaError_t e = cudaGetDeviceCount(&n);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *count = 0;
-    return PSG_OK;      // no driver / no device: zero devices
-  }
-  *count = n;
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!count) return fail(PSG_ERR_ARG, "count is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      *count = 0;
+      return PSG_OK;      // no driver / no device: zero devices
+    }
+    *count = n;
+    return PSG_OK;
+  });
 }
 
 int psg_device_describe(int index, char* buf, size_t len) {
-  if (!buf || len == 0) return fail(PSG_ERR_ARG, "buffer is NULL");
-  int n = 0;
-  psg_device_count(&n);
-  if (index < 0 || index >= n) return fail(PSG_ERR_NO_DEVICE, "GPU device index out of range");
-  cudaDeviceProp p;
-  if (cudaGetDeviceProperties(&p, index) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(PSG_ERR_CUDA, "cudaGetDeviceProperties failed");
-  }
-  std::snprintf(buf, len,
-                "[%d] CUDA: %s (CUDA compute %d.%d)\n"
-                "      %d compute units, %d MHz, %llu MiB global, %llu KiB local, max work-group %d",
-                index, p.name, p.major, p.minor, p.multiProcessorCount, p.clockRate / 1000,
-                (unsigned long long) (p.totalGlobalMem >> 20),
-                (unsigned long long) (p.sharedMemPerBlockOptin >> 10), p.maxThreadsPerBlock);
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!buf || len == 0) return fail(PSG_ERR_ARG, "buffer is NULL");
+    int n = 0;
+    psg_device_count(&n);
+    if (index < 0 || index >= n) return fail(PSG_ERR_NO_DEVICE, "GPU device index out of range");
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, index) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(PSG_ERR_CUDA, "cudaGetDeviceProperties failed");
+    }
+    std::snprintf(buf, len,
+                  "[%d] CUDA: %s (CUDA compute %d.%d)\n"
+                  "      %d compute units, %d MHz, %llu MiB global, %llu KiB local, max work-group %d",
+                  index, p.name, p.major, p.minor, p.multiProcessorCount, p.clockRate / 1000,
+                  (unsigned long long) (p.totalGlobalMem >> 20),
+                  (unsigned long long) (p.sharedMemPerBlockOptin >> 10), p.maxThreadsPerBlock);
+    return PSG_OK;
+  });
 }
 
 int psg_init(int device, const psg_config* cfg, psg_context** out) {
-  if (!out) return fail(PSG_ERR_ARG, "out is NULL");
-  *out = nullptr;
-  std::unique_ptr<psg_context> ctx(new (std::nothrow) psg_context());
-  if (!ctx) return fail(PSG_ERR_NOMEM, "cannot allocate context");
-  std::string err;
-  int rc = ctx->engine.init(device, to_engine(cfg), err);
-  if (rc) return fail(rc, err);
-  *out = ctx.release();
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!out) return fail(PSG_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    std::unique_ptr<psg_context> ctx(new (std::nothrow) psg_context());
+    if (!ctx) return fail(PSG_ERR_NOMEM, "cannot allocate context");
+    std::string err;
+    int rc = ctx->engine.init(device, to_engine(cfg), err);
+    if (rc) return fail(rc, err);
+    *out = ctx.release();
+    return PSG_OK;
+  });
 }
 
 void psg_destroy(psg_context* ctx) { delete ctx; }
 
 int psg_get_config(const psg_context* ctx, psg_config* out) {
-  if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
-  const psg::EngineConfig& c = ctx->engine.config();
-  std::memset(out, 0, sizeof *out);
-  out->seg_bytes = ctx->engine.seg_bytes();
-  out->block = ctx->engine.block();
-  out->ctas_per_sm = ctx->engine.grid() / (uint32_t) ctx->engine.props().multiProcessorCount;
-  out->small_limit = c.small_limit;
-  out->big_limit = c.big_limit;
-  out->window_segments = c.window_segments;
-  out->bucket_lists = c.bucket_lists;
-  out->presieve = c.presieve;
-  out->segments_per_launch = c.segments_per_launch;
-  out->sweep_limit = c.sweep_limit;
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !out) return fail(PSG_ERR_ARG, "NULL argument");
+    const psg::EngineConfig& c = ctx->engine.config();
+    std::memset(out, 0, sizeof *out);
+    out->seg_bytes = ctx->engine.seg_bytes();
+    out->block = ctx->engine.block();
+    out->ctas_per_sm = ctx->engine.grid() / (uint32_t) ctx->engine.props().multiProcessorCount;
+    out->small_limit = c.small_limit;
+    out->big_limit = c.big_limit;
+    out->window_segments = c.window_segments;
+    out->bucket_lists = c.bucket_lists;
+    out->presieve = c.presieve;
+    out->segments_per_launch = c.segments_per_launch;
+    out->sweep_limit = c.sweep_limit;
+    return PSG_OK;
+  });
 }
 
 int psg_describe(const psg_context* ctx, char* buf, size_t len) {
-  if (!ctx || !buf || !len) return fail(PSG_ERR_ARG, "NULL argument");
-  std::snprintf(buf, len, "%s", ctx->engine.describe().c_str());
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !buf || !len) return fail(PSG_ERR_ARG, "NULL argument");
+    std::snprintf(buf, len, "%s", ctx->engine.describe().c_str());
+    return PSG_OK;
+  });
 }
 
 int psg_count(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6]) {
-  if (!ctx || !counts) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  int rc = ctx->engine.count(start, stop, kinds, counts, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !counts) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.count(start, stop, kinds, counts, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
                     uint64_t* dev_counts, void* stream) {
-  if (!ctx || !dev_counts) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  int rc = ctx->engine.count_async(start, stop, kinds, reinterpret_cast<unsigned long long*>(dev_counts),
-                                   static_cast<cudaStream_t>(stream), err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !dev_counts) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.count_async(start, stop, kinds, reinterpret_cast<unsigned long long*>(dev_counts),
+                                     static_cast<cudaStream_t>(stream), err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n, uint64_t* counts) {
-  if (!ctx || (n && (!ranges || !counts))) return fail(PSG_ERR_ARG, "NULL argument");
-  static_assert(sizeof(psg_range) == sizeof(psg::RangeQuery) &&
-                offsetof(psg_range, start) == offsetof(psg::RangeQuery, start) &&
-                offsetof(psg_range, stop) == offsetof(psg::RangeQuery, stop) &&
-                offsetof(psg_range, kinds) == offsetof(psg::RangeQuery, kinds), "psg_range layout");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  int rc = ctx->engine.count_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, counts, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || (n && (!ranges || !counts))) return fail(PSG_ERR_ARG, "NULL argument");
+    static_assert(sizeof(psg_range) == sizeof(psg::RangeQuery) &&
+                  offsetof(psg_range, start) == offsetof(psg::RangeQuery, start) &&
+                  offsetof(psg_range, stop) == offsetof(psg::RangeQuery, stop) &&
+                  offsetof(psg_range, kinds) == offsetof(psg::RangeQuery, kinds), "psg_range layout");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.count_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, counts, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_generate_primes(psg_context* ctx, uint64_t start, uint64_t stop, uint64_t* out, size_t capacity,
                         size_t* count) {
-  if (!ctx || !count || (capacity && !out)) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  std::vector<uint64_t> v;
-  int rc = ctx->engine.generate_primes(start, stop, v, err);
-  if (rc) return fail(rc, err);
-  *count = v.size();
-  std::copy(v.begin(), v.begin() + std::min(v.size(), capacity), out);
-  if (capacity < v.size())
-    return fail(PSG_ERR_LIMIT, "output capacity " + std::to_string(capacity) + " < " + std::to_string(v.size()) + " primes");
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !count || (capacity && !out)) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    std::vector<uint64_t> v;
+    int rc = ctx->engine.generate_primes(start, stop, v, err);
+    if (rc) return fail(rc, err);
+    *count = v.size();
+    std::copy(v.begin(), v.begin() + std::min(v.size(), capacity), out);
+    if (capacity < v.size())
+      return fail(PSG_ERR_LIMIT, "output capacity " + std::to_string(capacity) + " < " + std::to_string(v.size()) + " primes");
+    return PSG_OK;
+  });
 }
 
 int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime) {
-  if (!ctx || !prime) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  int rc = ctx->engine.nth_prime(n, start, *prime, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !prime) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.nth_prime(n, start, *prime, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, double budget_seconds,
                        psg_tune_class* report, size_t cap, size_t* count) {
-  if (!ctx || (n && !ranges) || (cap && !report)) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  std::vector<psg::TuneReport> rep;
-  int rc = ctx->engine.autotune_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, budget_seconds, rep, err);
-  if (rc) return fail(rc, err);
-  if (count) *count = rep.size();
-  for (size_t i = 0; i < rep.size() && i < cap; i++) {
-    psg_tune_class& o = report[i];
-    o.range_class = rep[i].cls;
-    o.sample_ranges = (uint32_t) rep[i].sample_ranges;
-    o.sample_integers = rep[i].sample_integers;
-    o.direct_budget = rep[i].chosen.direct_budget;
-    o.big_limit = rep[i].chosen.big_limit;
-    o.stripe = rep[i].chosen.stripe;
-    o.best_seconds = rep[i].best_seconds;
-    o.default_seconds = rep[i].default_seconds;
-  }
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || (n && !ranges) || (cap && !report)) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    std::vector<psg::TuneReport> rep;
+    int rc = ctx->engine.autotune_batch(reinterpret_cast<const psg::RangeQuery*>(ranges), n, budget_seconds, rep, err);
+    if (rc) return fail(rc, err);
+    if (count) *count = rep.size();
+    for (size_t i = 0; i < rep.size() && i < cap; i++) {
+      psg_tune_class& o = report[i];
+      o.range_class = rep[i].cls;
+      o.sample_ranges = (uint32_t) rep[i].sample_ranges;
+      o.sample_integers = rep[i].sample_integers;
+      o.direct_budget = rep[i].chosen.direct_budget;
+      o.big_limit = rep[i].chosen.big_limit;
+      o.stripe = rep[i].chosen.stripe;
+      o.best_seconds = rep[i].best_seconds;
+      o.default_seconds = rep[i].default_seconds;
+    }
+    return PSG_OK;
+  });
 }
 
 int psg_prepare(psg_context* ctx, uint64_t stop) {
-  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::string err;
-  int rc = ctx->engine.prepare(stop, err);
-  return rc ? fail(rc, err) : PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.prepare(stop, err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
 }
 
 int psg_set_profiling(psg_context* ctx, int on) {
-  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  ctx->engine.set_profiling(on != 0);
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->engine.set_profiling(on != 0);
+    return PSG_OK;
+  });
 }
 
 int psg_kernel_stats(psg_context* ctx, const char** names, uint64_t* launches, double* ms,
                      size_t cap, size_t* n) {
-  if (!ctx || !n) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  std::vector<psg::KernelStat> st = ctx->engine.kernel_stats();
-  *n = st.size();
-  for (size_t i = 0; i < st.size() && i < cap; i++) {
-    if (names) names[i] = st[i].name;
-    if (launches) launches[i] = st[i].launches;
-    if (ms) ms[i] = st[i].ms;
-  }
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !n) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::vector<psg::KernelStat> st = ctx->engine.kernel_stats();
+    *n = st.size();
+    for (size_t i = 0; i < st.size() && i < cap; i++) {
+      if (names) names[i] = st[i].name;
+      if (launches) launches[i] = st[i].launches;
+      if (ms) ms[i] = st[i].ms;
+    }
+    return PSG_OK;
+  });
 }
 
 int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset) {
-  if (!ctx || !total) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  *total = ctx->engine.bucket_entries();
-  if (reset) ctx->engine.reset_bucket_entries();
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx || !total) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    *total = ctx->engine.bucket_entries();
+    if (reset) ctx->engine.reset_bucket_entries();
+    return PSG_OK;
+  });
 }
 
 int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s) {
-  if (!ctx || !atomics_per_s) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  *atomics_per_s = ctx->engine.measure_smem_atomic_rate();
-  return *atomics_per_s > 0 ? PSG_OK : fail(PSG_ERR_CUDA, "probe kernel failed");
+  return guarded([&]() -> int {
+    if (!ctx || !atomics_per_s) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    *atomics_per_s = ctx->engine.measure_smem_atomic_rate();
+    return *atomics_per_s > 0 ? PSG_OK : fail(PSG_ERR_CUDA, "probe kernel failed");
+  });
 }
 
 int psg_reset_kernel_stats(psg_context* ctx) {
-  if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lock(ctx->mu);
-  ctx->engine.reset_kernel_stats();
-  return PSG_OK;
+  return guarded([&]() -> int {
+    if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->engine.reset_kernel_stats();
+    return PSG_OK;
+  });
 }
 
 } // extern "C"
