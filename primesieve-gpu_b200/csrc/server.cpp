@@ -37,6 +37,11 @@ int Server::start(const ServerConfig& cfg, std::string& err) {
   if (!cfg_.prime_limit) cfg_.prime_limit = 0xffffffffull;
   {
     std::lock_guard<std::mutex> g(eng_mu_);
+    // whatever a failed start allocated is freed before it returns
+    struct Undo {
+      Server* s; bool armed = true;
+      ~Undo() { if (armed) s->release(); }
+    } undo{ this };
     SRV_CUDA(cudaSetDevice(eng_.device()));
     // resident sieving-prime table: every stop up to prime_limit^2
     const uint64_t lim = std::min<uint64_t>(cfg_.prime_limit, 0xffffffffull);
@@ -67,11 +72,23 @@ int Server::start(const ServerConfig& cfg, std::string& err) {
     SRV_CUDA(cudaMallocHost(&h_rows_, slots * 6 * sizeof(unsigned long long)));
     SRV_CUDA(cudaMalloc(&d_queue_, sizeof(uint32_t)));
     SRV_CUDA(cudaMallocHost(&h_flag_, sizeof(uint32_t)));
+    undo.armed = false;
   }
+  free_slots_.clear();
   for (int s = (int) cfg_.max_slots - 1; s >= 0; s--) free_slots_.push_back(s);
   stop_ = false;
-  started_ = true;
-  worker_ = std::thread([this] { loop(); });
+  try {
+    worker_ = std::thread([this] { loop(); });
+  } catch (...) {
+    std::lock_guard<std::mutex> g(eng_mu_);
+    free_slots_.clear();
+    release();
+    throw;
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    started_ = true;
+  }
   return PSG_OK;
 }
 
@@ -85,8 +102,12 @@ void Server::stop() {
   worker_.join();
   started_ = false;
   std::lock_guard<std::mutex> g(eng_mu_);
+  release();
+}
+
+void Server::release() {
   cudaSetDevice(eng_.device());
-  cudaStreamSynchronize(st_);
+  if (st_) cudaStreamSynchronize(st_);
   cudaFree(d_ranges_); cudaFree(d_rows_); cudaFree(d_items_); cudaFree(d_queue_);
   if (h_rows_) cudaFreeHost(h_rows_);
   if (h_flag_) cudaFreeHost(h_flag_);

@@ -85,6 +85,7 @@ private:
   };
 
   void loop();
+  void release();                  // free the device and pinned buffers (engine mutex held)
   int step(std::vector<Request*>& admitted, std::string& err);
   void finish(Request* r, int status, const std::string& err);
 
