@@ -224,7 +224,9 @@ int psg_server_start(psg_context* ctx, const psg_server_config* cfg, psg_server*
 /* Queue a count of [start, stop] (kinds mask); *id names it for wait. */
 int psg_server_submit(psg_server* s, uint64_t start, uint64_t stop, uint32_t kinds, uint64_t* id);
 /* Block until request id is done: counts[6] and its latency (seconds from
- * submit to completion). Returns the request's status. */
+ * submit to completion). Returns the request's status. Each id is collected
+ * by one wait: a second wait for it, concurrent or later, fails with
+ * PSG_ERR_ARG. */
 int psg_server_wait(psg_server* s, uint64_t id, uint64_t counts[6], double* latency_seconds);
 /* Load replay: submits requests[i] at arrival_seconds[i] after the call
  * (ascending), waits for all; counts is n x 6, latency from the scheduled

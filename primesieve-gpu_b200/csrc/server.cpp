@@ -147,6 +147,8 @@ int Server::wait(uint64_t id, uint64_t counts[6], double* latency_s, std::string
   auto it = reqs_.find(id);
   if (it == reqs_.end()) { err = "unknown request id " + std::to_string(id); return PSG_ERR_ARG; }
   Request* r = it->second.get();
+  if (r->claimed) { err = "request " + std::to_string(id) + " is already being waited for"; return PSG_ERR_ARG; }
+  r->claimed = true;
   cv_done_.wait(lk, [&] { return r->done; });
   if (counts) std::memcpy(counts, r->counts, 6 * sizeof(uint64_t));
   if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
@@ -169,12 +171,18 @@ int Server::replay(const RangeQuery* q, const double* arrival_s, size_t n, uint6
     std::this_thread::sleep_until(due(sent));
     rc = submit(q[sent].start, q[sent].stop, q[sent].kinds, ids[sent], err);
     if (rc) break;
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = reqs_.find(ids[sent]);
+    if (it != reqs_.end()) it->second->claimed = true;
   }
   for (size_t i = 0; i < sent; i++) {
-    std::string e;
     double lat = 0;
     std::unique_lock<std::mutex> lk(mu_);
     auto it = reqs_.find(ids[i]);
+    if (it == reqs_.end()) {              // collected by a wait() of its own
+      if (rc == PSG_OK) { rc = PSG_ERR_ARG; err = "request " + std::to_string(ids[i]) + " was collected elsewhere"; }
+      continue;
+    }
     Request* r = it->second.get();
     cv_done_.wait(lk, [&] { return r->done; });
     // latency from the scheduled arrival, so a late submission is not hidden

@@ -55,6 +55,7 @@ public:
   // Queue a count of [start, stop]; id identifies it for wait().
   int submit(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t& id, std::string& err);
   // Block until request id is done; counts overwritten, latency = done - submit.
+  // Each id is collected once: a second wait() for it fails with PSG_ERR_ARG.
   int wait(uint64_t id, uint64_t counts[6], double* latency_s, std::string& err);
   // Submit q[i] at arrival_s[i] seconds after the call (one thread paces the
   // arrivals), wait for all; latency[i] from the scheduled arrival.
@@ -71,6 +72,7 @@ private:
     uint64_t small[6] = { 0, 0, 0, 0, 0, 0 };   // 2/3/5 table (host)
     Clock::time_point t_submit, t_done;
     bool done = false;
+    bool claimed = false;                       // a wait() (or replay) collects it
     int status = 0;
     std::string err;
     uint64_t counts[6] = { 0, 0, 0, 0, 0, 0 };

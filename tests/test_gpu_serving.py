@@ -60,3 +60,30 @@ def test_server_refuses_over_hbm_budget(psg, ctx):
         assert e.value.status == 4 and "HBM budget" in str(e.value)
         assert srv.wait(small)[0] == ctx.count(10 ** 9, 10 ** 9 + 10 ** 6, 1)
         assert srv.stats()["refused"] == 1
+
+
+def test_server_each_id_collected_once(psg, ctx):
+    """Two waits for one request, concurrent or one after the other: exactly
+    one gets the counts, the other fails with PSG_ERR_ARG (1)."""
+    import threading
+    a, b = 10 ** 15, 10 ** 15 + 10 ** 10
+    want = ctx.count(a, b, 1)
+    with psg.Server(ctx) as srv:
+        rid = srv.submit(a, b, 1)
+        results = []
+
+        def waiter():
+            try:
+                results.append(srv.wait(rid)[0])
+            except psg.PsgError as e:
+                results.append(e.status)
+
+        threads = [threading.Thread(target=waiter) for _ in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert sorted(results, key=str) == sorted([want, 1], key=str)
+        with pytest.raises(psg.PsgError) as e:
+            srv.wait(rid)
+        assert e.value.status == 1
