@@ -88,6 +88,8 @@ int psg_device_describe(int index, char* buf, size_t len);
 /* ---- context ------------------------------------------------------------ */
 /* device < 0 picks the device with the most SMs. cfg may be NULL. */
 int psg_init(int device, const psg_config* cfg, psg_context** out);
+/* Stop every server started on ctx (psg_server_stop) before destroying it:
+ * a server's worker thread uses the context. */
 void psg_destroy(psg_context* ctx);
 /* The configuration actually in use (autotuned values filled in). */
 int psg_get_config(const psg_context* ctx, psg_config* out);

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 from typing import Iterable, List, Optional, Sequence, Tuple
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -153,12 +154,17 @@ class Context:
         _check(lib.psg_init(device, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._lib = lib
+        self._servers = weakref.WeakSet()     # servers running on this context
 
     @property
     def handle(self) -> ctypes.c_void_p:
         return self._h
 
     def close(self) -> None:
+        """Stops the context's servers (their worker threads use the
+        engine), then destroys the context."""
+        for srv in list(getattr(self, "_servers", ())):
+            srv.close()
         if self._h:
             self._lib.psg_destroy(self._h)
             self._h = None
@@ -269,7 +275,7 @@ class Context:
 
 class Server:
     """Request server with continuous batching on a context (psg_server_*).
-    The context must stay open while the server runs."""
+    The server keeps its context alive; closing the context stops it."""
 
     def __init__(self, ctx: "Context", **config: int):
         lib = load()
@@ -280,6 +286,8 @@ class Server:
         _check(lib.psg_server_start(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._lib = lib
+        self._ctx = ctx                       # the context outlives the server
+        ctx._servers.add(self)
 
     def submit(self, start: int, stop: int, kinds: int = 0x3F) -> int:
         rid = ctypes.c_uint64(0)
@@ -319,6 +327,12 @@ class Server:
 
     def __exit__(self, *exc) -> None:
         self.close()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def serving_workload(n: int, rate: float, seed: int = 1, len_log2: Tuple[float, float] = (12.0, 36.0),

@@ -87,3 +87,17 @@ def test_server_each_id_collected_once(psg, ctx):
         with pytest.raises(psg.PsgError) as e:
             srv.wait(rid)
         assert e.value.status == 1
+
+
+def test_closing_the_context_stops_its_server(psg):
+    """A server keeps its context alive and closing the context stops the
+    server first (its worker thread uses the engine)."""
+    c = psg.Context()
+    srv = psg.Server(c)
+    rid = srv.submit(10 ** 12, 10 ** 12 + 10 ** 8, 1)
+    assert srv.wait(rid)[0][0] == c.count(10 ** 12, 10 ** 12 + 10 ** 8, 1)[0]
+    c.close()
+    assert srv._h is None
+    with pytest.raises(psg.PsgError) as e:
+        srv.submit(0, 100, 1)      # stopped: a NULL server handle
+    assert e.value.status == 1
