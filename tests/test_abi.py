@@ -65,6 +65,38 @@ def test_no_device_fails_loudly(psg):
     assert ctypes.get_errno() == 33          # EDOM
 
 
+def test_null_handles_are_argument_errors(psg):
+    """Every psg_* entry point that takes a context or server turns a NULL
+    handle into PSG_ERR_ARG (1) with a message; none crashes or throws
+    (no GPU needed: the check comes before any device work)."""
+    lib = psg.load()
+    u64 = ctypes.c_uint64
+    out6 = (u64 * 6)()
+    rid = u64(0)
+    d = ctypes.c_double(0)
+    n = ctypes.c_size_t(0)
+    calls = {
+        "psg_count": lambda: lib.psg_count(None, 0, 100, 63, out6),
+        "psg_count_async": lambda: lib.psg_count_async(None, 0, 100, 63, out6, None),
+        "psg_count_batch": lambda: lib.psg_count_batch(None, None, 0, None),
+        "psg_nth_prime": lambda: lib.psg_nth_prime(None, 1, 0, ctypes.byref(rid)),
+        "psg_generate_primes": lambda: lib.psg_generate_primes(None, 0, 100, None, 0, ctypes.byref(n)),
+        "psg_prepare": lambda: lib.psg_prepare(None, 100),
+        "psg_set_profiling": lambda: lib.psg_set_profiling(None, 1),
+        "psg_reset_kernel_stats": lambda: lib.psg_reset_kernel_stats(None),
+        "psg_bucket_entries": lambda: lib.psg_bucket_entries(None, ctypes.byref(rid), 0),
+        "psg_server_start": lambda: lib.psg_server_start(None, None, ctypes.byref(ctypes.c_void_p())),
+        "psg_server_submit": lambda: lib.psg_server_submit(None, 0, 100, 1, ctypes.byref(rid)),
+        "psg_server_wait": lambda: lib.psg_server_wait(None, 1, out6, ctypes.byref(d)),
+        "psg_server_replay": lambda: lib.psg_server_replay(None, None, None, 0, None, None),
+    }
+    for name, call in calls.items():
+        assert call() == 1, name
+        assert lib.psg_last_error(), name
+    lib.psg_server_stop(None)          # no-ops
+    lib.psg_destroy(None)
+
+
 def cli(*args):
     return subprocess.run([os.path.join(PKG_DIR, "bin", "primesieve"), *args], capture_output=True, text=True)
 
