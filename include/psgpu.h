@@ -21,6 +21,18 @@
  *                        src/gpu/GpuSieve.cpp:43-72.
  *   psg_config fields    GpuConfig src/gpu/GpuBackend.hpp:45-58 and the
  *                        set_gpu_* knobs include/primesieve/gpu.hpp:48-53.
+ *   psg_get_config / psg_describe  GpuBackend::sieveBytes(), workGroupSize(),
+ *                        device() src/gpu/GpuBackend.hpp:64, :72-73 and
+ *                        gpu_active_device() include/primesieve/gpu.hpp:57.
+ *   psg_last_error       gpu_last_error() include/primesieve/gpu.hpp:60
+ *                        (here per thread; psg_status_string has no
+ *                        counterpart: the reference throws primesieve_error).
+ *   psg_version          primesieve_version() include/primesieve.h:243.
+ *   psg_generate_primes, psg_nth_prime  cited at their declarations below.
+ *   psg_count_async, psg_prepare, psg_autotune_batch, psg_server_*, the
+ *   profiling calls and psg_count_noalloc  no counterpart (the reference
+ *                        counts one range per synchronous call,
+ *                        src/api.cpp:48-118, and has no device-side API).
  */
 #ifndef PSGPU_H
 #define PSGPU_H
