@@ -37,7 +37,7 @@ def worker(rank, world, port, cases, q):
     q.put((rank, res))
 
 
-@pytest.mark.parametrize("world", [2])
+@pytest.mark.parametrize("world", [2, 3])
 def test_sharded_counts_match(world, oracle, ref_counts):
     cases = [(0, 10 ** 6), (999999900, 1000000331), (10 ** 12, 10 ** 12 + 3 * 10 ** 5), (0, 40), (7, 7)]
     ctx = mp.get_context("spawn")
