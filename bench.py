@@ -17,9 +17,21 @@ e2e   : the same metric through the C ABI call psg_count() with host
         arguments and a host result (launches, accumulator reset and the
         device->host copy inside the timed region), wall clock, max over ranks.
 --impl reference : the reference's own CPU sieve (oracle/_ref/primesieve,
-        built from the reference sources) on all host cores, on bounded
-        samples of the same workload; the C restatement in oracle/ stands in
-        if that binary is missing.
+        built from the reference sources) on all host cores, one full pass of
+        the same workload per step (a bounded sample if the host is too slow
+        for the run to end within a few minutes); the C restatement in
+        oracle/ stands in if that binary is missing.
+
+Besides the headline line's own workload, one GPU (N=1) also reports:
+configs  : pi(1e9), the six counts of [0, 1e11] and of [2^64-2^34, 2^64-1],
+           each device-timed, end to end through psg_count, and with the
+           reference CLI's time on the full range in the same run;
+serving  : the seed-1 request stream (lengths 2^12..2^36, starts up to
+           1.8e19, kinds 1..6) replayed through psg_server_replay at
+           100 .. 50k requests/s: p50/p99 latency and integers/s per rate,
+           beside the reference library replaying a seeded sample of it;
+batched  : the 4096-range workload through psg_count_batch vs one psg_count
+           per range, beside the reference library on a sample of it.
 """
 import argparse
 import json
@@ -42,6 +54,27 @@ GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
 # 667.471872 MB read + 6.376192 MB written
 FILL_DRAM_BYTES_PER_ENTRY = (612.604416e6 + 67.080192e6) / 167958746
 SIEVE_DRAM_BYTES_PER_ENTRY = (667.471872e6 + 6.376192e6) / 167958746
+
+
+CONFIGS = [
+    # (name, start, stop, kinds mask, reference CLI count flags)
+    ("pi(1e9)", 0, 10 ** 9, 0x01, "-c1"),
+    ("counts 1-6 of [0, 1e11]", 0, 10 ** 11, 0x3F, "-c123456"),
+    ("counts 1-6 of [2^64-2^34, 2^64-1]", 2 ** 64 - 2 ** 34, 2 ** 64 - 1, 0x3F, "-c123456"),
+]
+GOLDEN_COUNTS = os.path.join(REPO, "tests", "golden", "ref_counts.json")
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def env_rank():
@@ -160,31 +193,46 @@ def reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    # per step: one bounded sample of the workload sized to ~6 s of CPU work,
-    # less when many steps are asked for (the whole run stays near 90 s)
-    rate, n, el, kind, cores = cpu_reference_rate(max(1.0, min(6.0, 90.0 / (args.warmup + args.steps))))
     exe = os.path.join(REPO, "oracle", "_ref", "primesieve")
-    times = []
-    for i in range(args.warmup + args.steps):
-        t = time.perf_counter()
-        if kind == "reference":
+    cores = os.cpu_count() or 1
+    steps = args.warmup + args.steps
+    if os.path.exists(exe):
+        kind = "reference"
+
+        def run(n):
             subprocess.run([exe, str(START), str(START + n), "-c1", "-q", "-t", str(cores)],
                            capture_output=True, check=True)
-        else:
-            sys.path.insert(0, os.path.join(REPO, "tests"))
-            from conftest import Oracle
-            Oracle().plain(START, START + n, 1)
+        # one full pass of the workload per step when the whole run fits in
+        # about three minutes on this host, else the largest sample that does
+        t = time.perf_counter()
+        run(LENGTH)
+        full_s = time.perf_counter() - t
+        n = LENGTH if full_s * steps <= 180.0 else max(10 ** 9, int(LENGTH * 180.0 / (full_s * steps)))
+    else:
+        kind, cores = "port", 1
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        from conftest import Oracle     # the C restatement, single-threaded
+        orc = Oracle()
+
+        def run(n):
+            orc.plain(START, START + n, 1)
+        n = 10 ** 9
+    times = []
+    for i in range(steps):
+        t = time.perf_counter()
+        run(n)
         if i >= args.warmup:
             times.append(time.perf_counter() - t)
     total = sum(times)
     value = n * len(times) / total
+    sample = f"[1e15, 1e15+{n:.3g}] per step, -t {cores}"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "sample": f"[1e15, 1e15+{n:.3g}] per step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"[1e15, 1e15+{n:.3g}] per step, -t {cores}"},
+        "data": "synthetic", "config": {"workload": WORKLOAD, "sample": sample, "full_range": n == LENGTH},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -199,6 +247,9 @@ def main():
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-per-range section")
+    ap.add_argument("--no-configs", action="store_true", help="skip the per-config section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    ap.add_argument("--serving-requests", type=int, default=1000, help="requests per serving rate")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -254,6 +305,13 @@ def main():
     barrier()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
+    # the asynchronous passes cannot recount: every one of them must have
+    # kept all of its bucket entries
+    try:
+        ctx.count_async_status()
+        async_exact = True
+    except psg.PsgError:
+        async_exact = False
     stats = ctx.kernel_stats()
     launches = sum(v[0] for v in stats.values())
     entries = ctx.bucket_entries(reset=True)
@@ -273,7 +331,7 @@ def main():
     torch.cuda.synchronize()
     kst = ctx.kernel_stats()
     ctx.set_profiling(False)
-    smem_rate = ctx.smem_atomic_rate()
+    smem_rand, smem_cf = ctx.smem_atomic_rates()
     hbm_peak, peak_src = load_peaks()
     entries_per_pass = entries / args.steps
     sieve_l, sieve_ms = kst.get("sieve_count_kernel", (0, 0.0))
@@ -307,10 +365,12 @@ def main():
                   "traffic_source": "ncu dram__bytes_read+write per entry on a one-window case, scaled",
                   "algorithmic_bytes_per_launch": sieve_bytes / max(sieve_l, 1),
                   "avg_launch_ms": sieve_ms / max(sieve_l, 1), "peak_source": peak_src,
-                  "limit": {"bound": "smem_atomic", "achieved": sieve_rate / 1e9, "peak": smem_rate / 1e9,
-                            "unit": "Gatomic/s", "frac": sieve_rate / max(smem_rate, 1),
-                            "crossings_per_pass": crossings, "bucket_entries_applied_per_pass": entries_per_pass,
-                            "peak_source": "measured in-run (random-address smem atomicAnd probe)"}}
+                  "limit": {"bound": "smem_atomic", "achieved": sieve_rate / 1e9, "unit": "Gatomic/s",
+                            "peak": smem_cf / 1e9, "frac": sieve_rate / max(smem_cf, 1),
+                            "peak_source": "measured in-run: conflict-free smem atomicAnd probe (lane l on bank l)",
+                            "peak_random": smem_rand / 1e9, "frac_random": sieve_rate / max(smem_rand, 1),
+                            "peak_random_source": "measured in-run: random-address smem atomicAnd probe",
+                            "crossings_per_pass": crossings, "bucket_entries_applied_per_pass": entries_per_pass}}
 
     # ---- end to end through the C ABI with host buffers ----------------------
     # psg_count: host arguments in, host counts out (launches, the device
@@ -329,14 +389,20 @@ def main():
     tot = torch.tensor([got0], dtype=torch.int64, device="cuda")
     if world > 1:
         dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    ok0 = (rank != 0) or (got0 == GOLDEN_1E15 and e2e_count == GOLDEN_1E15)
+    ok0 = async_exact and ((rank != 0) or (got0 == GOLDEN_1E15 and e2e_count == GOLDEN_1E15))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, n, el, kind, cores = cpu_reference_rate(12.0)
-        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": kind,
                "sample": f"[1e15, 1e15+{n:.3g}] in {el:.1f} s, -t {cores}"}
 
+    configs = None
+    if world == 1 and not args.no_configs:
+        configs = config_section(psg, ctx, stream, args, torch)
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = serving_section(psg, ctx, args)
     batched = None
     if not args.no_batch:
         batched = batch_section(psg, ctx, rank, world, args, torch, dist)
@@ -346,11 +412,12 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "range_per_gpu": [a, b], "kinds": "primes",
                        "segment_bytes": cfg["seg_bytes"], "block": cfg["block"],
                        "l2": "inputs larger than L2: each pass streams %.1f GB of bucket lists" % (8 * entries_per_pass / 1e9),
-                       "count_ok": bool(ok0), "total_count": int(tot.item())},
+                       "count_ok": bool(ok0), "async_passes_exact": async_exact,
+                       "total_count": int(tot.item())},
             "roofline": roof_fill if dominant == "bucket_fill_kernel" else roof_sieve,
             "rooflines": [roof_sieve, roof_fill],
             "kernel_ms_per_pass": {k: v[1] for k, v in kst.items()},
@@ -359,6 +426,8 @@ def main():
                     "api": "psg_count (C ABI, host result)"},
             "gpu_launches": launches,
             "clocks": clk,
+            "configs": configs,
+            "serving": serving,
             "batched": batched,
         }
         print(json.dumps(line), flush=True)
@@ -366,7 +435,163 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
-    return 0 if ok0 else 1
+    ok_all = ok0 and all(c["count_ok"] for c in (configs or [])) and (serving is None or serving["count_ok"]) \
+        and (batched is None or batched["count_ok"])
+    return 0 if ok_all else 1
+
+
+def cli_seconds(start, stop, flag):
+    """The reference CLI (oracle/_ref/primesieve) on [start, stop] with all
+    host threads: (seconds, counts in -c order) or None without the binary."""
+    exe = os.path.join(REPO, "oracle", "_ref", "primesieve")
+    if not os.path.exists(exe):
+        return None
+    cores = os.cpu_count() or 1
+    t = time.perf_counter()
+    out = subprocess.run([exe, str(start), str(stop), flag, "-t", str(cores)], capture_output=True, text=True,
+                         check=True).stdout
+    el = time.perf_counter() - t
+    counts = [int(x.rsplit(":", 1)[1]) for x in out.strip().split("\n") if ":" in x and not x.startswith("Sec")]
+    return el, counts, cores
+
+
+def config_section(psg, ctx, stream, args, torch):
+    """The other single-range configurations: device-timed passes of
+    psg_count_async (CUDA events on the launch stream), the same count end to
+    end through psg_count, and the reference CLI on the full range."""
+    with open(GOLDEN_COUNTS) as f:
+        golden = {(r["start"], r["stop"]): r["counts"] for r in json.load(f)["bench"]}
+    hbm_peak, _ = load_peaks()
+    out = []
+    counts = torch.zeros(6, dtype=torch.int64, device="cuda")
+    for name, a, b, kinds, flag in CONFIGS:
+        ints = b - a + 1
+        ctx.prepare(b)
+
+        def step():
+            counts.zero_()
+            ctx.count_async(a, b, kinds, counts.data_ptr(), stream.cuda_stream)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        # about half a second of timed passes, at least 3
+        t = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        one = time.perf_counter() - t
+        k = max(3, min(200, int(0.5 / max(one, 1e-4))))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(k):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / k
+        try:
+            ctx.count_async_status()
+            exact_async = True
+        except psg.PsgError:
+            exact_async = False
+        dev_counts = [int(x) for x in counts.tolist()]
+        # end to end: host arguments in, host counts out
+        ctx.count(a, b, kinds)
+        ke = max(3, k // 2)
+        t = time.perf_counter()
+        for _ in range(ke):
+            host = ctx.count(a, b, kinds)
+        te = (time.perf_counter() - t) / ke
+        want = [c if (kinds >> i) & 1 else 0 for i, c in enumerate(golden[(a, b)])]
+        ok = exact_async and dev_counts == want and host == want
+        line = {"workload": f"{name}: [{a}, {b}]", "kinds": kinds, "value": ints / (ms * 1e-3), "unit": UNIT,
+                "ms_per_pass": ms, "passes": k, "counts": host, "count_ok": ok,
+                "e2e": {"value": ints / te, "unit": UNIT, "ms_per_call": te * 1e3,
+                        "h2d_bytes_per_step": 16, "d2h_bytes_per_step": 52, "api": "psg_count (C ABI, host result)"}}
+        if not args.no_cpu_baseline:
+            r = cli_seconds(a, b, flag)
+            if r:
+                el, cc, cores = r
+                line["cpu_baseline"] = {"value": ints / el, "unit": UNIT, "cores": cores, "cpu": cpu_model(),
+                                        "kind": "reference", "seconds": el,
+                                        "sample": f"full range, reference CLI {flag} -t {cores}"}
+                line["cpu_counts_match"] = cc == [want[i] for i in range(6) if (kinds >> i) & 1]
+                line["vs_cpu"] = line["e2e"]["value"] / line["cpu_baseline"]["value"]
+        out.append(line)
+    return out
+
+
+def serving_section(psg, ctx, args):
+    """The seed-1 serving stream replayed through one request server
+    (psg_server_replay paces the arrivals from C++; latency from each
+    request's scheduled arrival to its completion) at each rate, the same
+    requests at every rate. Throughput = integers of all requests / (last
+    completion - first arrival). A seeded sample of the results is checked
+    against psg_count."""
+    import random
+    import numpy as np
+    n = args.serving_requests
+    rates = [100.0, 1000.0, 10000.0, 50000.0]
+    rows = []
+    ok = True
+    with psg.Server(ctx) as srv:
+        for rate in rates:
+            reqs, arr = psg.serving_workload(n, rate, seed=1)
+            ints = float(sum(b - a + 1 for a, b, _ in reqs))
+            t = time.perf_counter()
+            res, lats = srv.replay(reqs, arr)
+            wall = time.perf_counter() - t
+            lat = np.array(lats)
+            span = max(wall, 1e-9)
+            rows.append({"rate": rate, "requests": n, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                         "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3),
+                         "integers": ints, "value": ints / span, "unit": UNIT,
+                         "offered": ints / max(arr[-1], 1e-9), "seconds": wall})
+            for i in random.Random(int(rate)).sample(range(n), 8):
+                a, b, k = reqs[i]
+                ok = ok and res[i] == ctx.count(a, b, k)
+        st = srv.stats()
+    out = {"workload": "serving stream seed 1: Poisson arrivals, start log-uniform [1e6, 1.8e19], length "
+                       "log-uniform [2^12, 2^36], kind uniform over 1..6",
+           "api": "psg_server_replay (C ABI)", "rates": rows, "count_ok": ok,
+           "sustained": max(rows, key=lambda r: r["value"]),
+           "server": {k: st[k] for k in ("steps", "bucket_requests", "batch_requests", "refused")}}
+    if not args.no_cpu_baseline:
+        reqs, _ = psg.serving_workload(n, 1000.0, seed=1)
+        out["cpu_baseline"] = cpu_trace_rate(reqs, 10.0)
+    return out
+
+
+def cpu_trace_rate(reqs, budget_s):
+    """The reference library replaying a seeded sample of a request trace, one
+    count call per request with all host threads; stops after budget_s."""
+    import ctypes
+    import random
+    lib_path = os.path.join(REPO, "oracle", "_ref", "libprimesieve_ref.so")
+    if not os.path.exists(lib_path):
+        return None
+    lib = ctypes.CDLL(lib_path)
+    cores = os.cpu_count() or 1
+    lib.primesieve_set_num_threads.argtypes = [ctypes.c_int]
+    lib.primesieve_set_num_threads(cores)
+    fns = []
+    for name in ("primes", "twins", "triplets", "quadruplets", "quintuplets", "sextuplets"):
+        f = getattr(lib, "primesieve_count_" + name)
+        f.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        f.restype = ctypes.c_uint64
+        fns.append(f)
+    order = list(range(len(reqs)))
+    random.Random(0).shuffle(order)
+    done, ints, t0 = 0, 0, time.perf_counter()
+    for i in order:
+        a, b, k = reqs[i]
+        fns[k.bit_length() - 1](a, b)
+        done += 1
+        ints += b - a + 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": ints / el, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "reference",
+            "sample": f"{done} of {len(reqs)} requests (seeded shuffle), {ints:.3g} integers in {el:.1f} s"}
 
 
 BATCH_FIXTURE = os.path.join(REPO, "tests", "golden", "batch4096.json")
@@ -375,13 +600,13 @@ BATCH_WORKLOAD = ("4096 ranges, seed 0: start log-uniform [1e6, 1e16], length lo
 
 
 def batch_section(psg, ctx, rank, world, args, torch, dist):
-    """Batched vs per-range on the 4096-range workload (rank r takes ranges
-    i = r mod N). Both arms go through the C ABI with host arguments and host
+    """Batched vs per-range on the 4096-range workload (each rank takes an
+    equal share of the estimated work, psg.balance_ranges). Both arms go through the C ABI with host arguments and host
     results: per-range = one psg_count() per range, batched = one
     psg_count_batch() for all of them. Wall clock, max over ranks."""
     with open(BATCH_FIXTURE) as f:
         rows = json.load(f)["ranges"]
-    mine = [r for i, r in enumerate(rows) if i % world == rank]
+    mine = [rows[i] for i in psg.balance_ranges([(a, b) for a, b, _, _ in rows], world)[rank]]
     q = [(a, b, 1 << k) for a, b, k, _ in mine]
     ints = sum(b - a + 1 for a, b, _, _ in rows)
     ctx.prepare(max(b for _, b, _, _ in rows))
@@ -478,7 +703,7 @@ def cpu_batch_rate(rows, budget_s):
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    return {"value": ints / el, "unit": UNIT, "cores": cores, "kind": "reference",
+    return {"value": ints / el, "unit": UNIT, "cores": cores, "cpu": cpu_model(), "kind": "reference",
             "sample": f"{done} of {len(rows)} ranges (seeded shuffle), {ints:.3g} integers in {el:.1f} s"}
 
 

@@ -7,8 +7,11 @@
  * the functions print a message to stderr, set errno to EDOM and return
  * PRIMESIEVE_ERROR, exactly like the reference.
  *
- * The reference's prime generation, printing and nth-prime functions are not
- * part of this library (counting path only).
+ * Prime generation (primesieve_generate_primes, primesieve_generate_n_primes)
+ * and primesieve_nth_prime are declared below too; they run on the GPU as
+ * well (the sieve keeps its segments as bitmaps, a kernel turns them into
+ * values). The iterator, printing and the RiemannR functions are not part
+ * of this library.
  */
 #ifndef PRIMESIEVE_H
 #define PRIMESIEVE_H

@@ -28,8 +28,10 @@
  *                        (here per thread; psg_status_string has no
  *                        counterpart: the reference throws primesieve_error).
  *   psg_version          primesieve_version() include/primesieve.h:243.
- *   psg_generate_primes, psg_nth_prime  cited at their declarations below.
- *   psg_count_async, psg_prepare, psg_autotune_batch, psg_server_*, the
+ *   psg_generate_primes, psg_nth_prime, psg_sieving_primes  cited at their
+ *                        declarations below.
+ *   psg_count_async, psg_count_async_status, psg_prepare,
+ *   psg_autotune_batch, psg_server_*, the
  *   profiling calls and psg_count_noalloc  no counterpart (the reference
  *                        counts one range per synchronous call,
  *                        src/api.cpp:48-118, and has no device-side API).
@@ -53,7 +55,8 @@ typedef enum {
   PSG_ERR_LIMIT = 5,      /* request beyond a documented maximum */
   PSG_ERR_INTERNAL = 6,   /* internal consistency check failed */
   PSG_ERR_TIMEOUT = 7,    /* a bounded wait gave up */
-  PSG_ERR_CLOSED = 8      /* the server / queue has been shut down */
+  PSG_ERR_CLOSED = 8,     /* the server / queue has been shut down */
+  PSG_ERR_OVERFLOW = 9    /* an asynchronous count dropped bucket entries: recount */
 } psg_status;
 
 /* Count kinds: bit i of a kinds mask selects counts[i]. */
@@ -81,7 +84,9 @@ typedef struct {
   uint32_t bucket_lists;       /* bucket lists per segment */
   uint32_t presieve;           /* pre-sieve with pattern tables: 0 = default (on), 1 = on, 2 = off */
   uint32_t segments_per_launch;/* cap on segments per launch (reference knob) */
-  uint32_t sweep_limit;        /* big primes below: segment-major bucket sweep */
+  uint32_t list_capacity_pct;  /* bucket-list capacity in % of the engine's estimate
+                                  (0 = 100); values below 100 make lists overflow, for
+                                  tests of the overflow handling */
 } psg_config;
 
 /* A [start, stop] range and the kinds wanted for it (batch API). */
@@ -118,12 +123,22 @@ int psg_count(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
  * 6 x uint64_t) on `stream` (a cudaStream_t, NULL = the context's stream).
  * The 2/3/5 table is included. Host-side preparation (the sieving-prime
  * table for sqrt(stop)) happens before return. Unlike psg_count it cannot
- * recount when a bucket list overflows. The lists are sized for their
- * expected length plus 6 sigma plus 32 entries, which no checked workload
- * has exceeded; psg_count detects an overflow and recounts with larger
- * lists. */
+ * recount when a bucket list overflows (the lists are sized for their
+ * expected length plus 6 sigma plus 32 entries): an overflow drops entries,
+ * so the counts written are too high. The kernels record it in the
+ * context, and psg_count_async_status() reports it: call it before
+ * trusting asynchronous counts. */
 int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t kinds,
                     uint64_t* dev_counts, void* stream);
+
+/* Waits for every count enqueued on the context so far and reports whether
+ * the psg_count_async calls since the previous status call were exact:
+ * PSG_OK, or PSG_ERR_OVERFLOW if a bucket list of one of them overflowed
+ * (its counts are too high; the lists have grown, so counting again gives
+ * the exact values). Clears the recorded state. No reference counterpart:
+ * the reference's GPU count is synchronous and surfaces every failure of
+ * its launch (src/gpu/GpuSieve.cpp:341-365). */
+int psg_count_async_status(psg_context* ctx);
 
 /* Count n ranges; counts is n x 6 (row i for ranges[i]). */
 int psg_count_batch(psg_context* ctx, const psg_range* ranges, size_t n,
@@ -169,6 +184,16 @@ int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, doub
 /* Build the sieving-prime table up to sqrt(stop) ahead of time. */
 int psg_prepare(psg_context* ctx, uint64_t stop);
 
+/* The device sieving-prime table, for tests and diagnostics. Replaces the
+ * reference's CPU generate_primes(7, sqrt(hi)) and upload
+ * (src/gpu/cuda/CudaBackend.cpp:346-388): psg_prepare(stop), then entries
+ * [first, first + n) of the table (clipped to its length) are copied to out
+ * (host). *total = the table's length; it holds, ascending, the primes p
+ * with *lo_excl < p <= *hi_incl (the pre-sieve primes are not in it; the
+ * table may reach beyond sqrt(stop), it grows geometrically). */
+int psg_sieving_primes(psg_context* ctx, uint64_t stop, size_t first, uint32_t* out, size_t n,
+                       size_t* total, uint64_t* lo_excl, uint64_t* hi_incl);
+
 /* ---- diagnostics -------------------------------------------------------- */
 const char* psg_last_error(void);
 const char* psg_status_string(int status);
@@ -183,14 +208,18 @@ int psg_reset_kernel_stats(psg_context* ctx);
 /* Bucket-sieve entries written (4 bytes each) since the last reset; waits for
  * the context's stream. reset != 0 zeroes the counter afterwards. */
 int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset);
-/* Roofline denominator of the cross-off phase: the measured rate of
- * random-address shared-memory atomicAnd on this device (atomics/s). */
-int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s);
+/* Roofline denominators of the cross-off phases, measured on this device
+ * (atomics/s): shared-memory atomicAnd at random addresses (a warp's lanes
+ * on banks at random, as in the medium, direct and bucket phases) and
+ * conflict-free (every lane on its own bank: the ceiling). conflict_free
+ * may be NULL. */
+int psg_measure_smem_atomic_rate(psg_context* ctx, double* random_addr, double* conflict_free);
 
 /* Count without allocating anything (no reference counterpart: the
  * reference always allocates through its backend). For callers that cannot
- * allocate device memory when they count -- inside CUDA graph capture,
- * allocator callbacks, real-time loops, fixed-budget embedders. Same result
+ * allocate device memory when they count: an allocator's own callbacks (a
+ * cudaMalloc there re-enters the allocator), real-time loops (a cudaMalloc
+ * can synchronise the device), embedders with a fixed memory budget. Same result
  * as psg_count(), written (overwritten) to dev_counts, a device buffer of 6
  * uint64_t, on `stream` (a cudaStream_t; NULL = the legacy default stream).
  * Runs on the current device; no context is needed.
@@ -248,6 +277,11 @@ int psg_server_wait(psg_server* s, uint64_t id, uint64_t counts[6], double* late
 int psg_server_replay(psg_server* s, const psg_range* requests, const double* arrival_seconds,
                       size_t n, uint64_t* counts, double* latency_seconds);
 int psg_server_get_stats(psg_server* s, psg_server_stats* out);
+/* For tests of the failure handling, on the host (no reference counterpart):
+ * the nth request the worker plans from now on (nth >= 1; 0 cancels) makes
+ * its step fail with `status`, as a failed CUDA call at that point would.
+ * Every request of that step, planned or not, completes with `status`. */
+int psg_server_inject_failure(psg_server* s, uint32_t nth, int status);
 /* Stops the worker (requests still queued fail with PSG_ERR_CLOSED). */
 void psg_server_stop(psg_server* s);
 

@@ -31,7 +31,8 @@ PSG_SYMBOLS = (
     "psg_bucket_entries", "psg_measure_smem_atomic_rate", "psg_count_noalloc",
     "psg_server_start", "psg_server_submit", "psg_server_wait", "psg_server_replay",
     "psg_server_get_stats", "psg_server_stop", "psg_generate_primes", "psg_nth_prime",
-    "psg_autotune_batch",
+    "psg_autotune_batch", "psg_count_async_status", "psg_server_inject_failure",
+    "psg_sieving_primes",
 )
 
 
@@ -46,7 +47,7 @@ class PsgError(RuntimeError):
 class PsgConfig(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in (
         "seg_bytes", "block", "ctas_per_sm", "small_limit", "big_limit",
-        "window_segments", "bucket_lists", "presieve", "segments_per_launch", "sweep_limit")]
+        "window_segments", "bucket_lists", "presieve", "segments_per_launch", "list_capacity_pct")]
 
 
 class PsgRange(ctypes.Structure):
@@ -96,8 +97,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_describe.argtypes = [vp, ctypes.c_char_p, sz]
     lib.psg_count.argtypes = [vp, u64, u64, u32, U64P]
     lib.psg_count_async.argtypes = [vp, u64, u64, u32, vp, vp]
+    lib.psg_count_async_status.argtypes = [vp]
     lib.psg_count_batch.argtypes = [vp, ctypes.POINTER(PsgRange), sz, U64P]
     lib.psg_prepare.argtypes = [vp, u64]
+    lib.psg_sieving_primes.argtypes = [vp, u64, sz, ctypes.POINTER(ctypes.c_uint32), sz,
+                                       ctypes.POINTER(sz), U64P, U64P]
     lib.psg_last_error.restype = ctypes.c_char_p
     lib.psg_status_string.restype = ctypes.c_char_p
     lib.psg_status_string.argtypes = [i32]
@@ -106,7 +110,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                      ctypes.POINTER(ctypes.c_double), sz, ctypes.POINTER(sz)]
     lib.psg_reset_kernel_stats.argtypes = [vp]
     lib.psg_bucket_entries.argtypes = [vp, U64P, i32]
-    lib.psg_measure_smem_atomic_rate.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    lib.psg_measure_smem_atomic_rate.argtypes = [vp, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(ctypes.c_double)]
     lib.psg_count_noalloc.argtypes = [u64, u64, u32, vp, vp]
     lib.psg_version.restype = ctypes.c_char_p
     DP = ctypes.POINTER(ctypes.c_double)
@@ -115,6 +120,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.psg_server_wait.argtypes = [vp, u64, U64P, DP]
     lib.psg_server_replay.argtypes = [vp, ctypes.POINTER(PsgRange), DP, sz, U64P, DP]
     lib.psg_server_get_stats.argtypes = [vp, ctypes.POINTER(PsgServerStats)]
+    lib.psg_server_inject_failure.argtypes = [vp, u32, i32]
     lib.psg_server_stop.argtypes = [vp]
     lib.psg_server_stop.restype = None
     lib.psg_generate_primes.argtypes = [vp, u64, u64, U64P, sz, ctypes.POINTER(sz)]
@@ -202,6 +208,12 @@ class Context:
                                          ctypes.c_void_p(dev_counts_ptr),
                                          ctypes.c_void_p(stream_ptr or None)))
 
+    def count_async_status(self) -> None:
+        """Waits for the counts enqueued so far; raises PsgError (status 9,
+        PSG_ERR_OVERFLOW) if an asynchronous count since the last call
+        dropped bucket entries, so that its counts are too high."""
+        _check(self._lib.psg_count_async_status(self._h))
+
     def count_batch(self, ranges: Sequence[Tuple[int, int, int]]) -> List[List[int]]:
         n = len(ranges)
         arr = (PsgRange * max(n, 1))()
@@ -247,6 +259,16 @@ class Context:
     def prepare(self, stop: int) -> None:
         _check(self._lib.psg_prepare(self._h, stop))
 
+    def sieving_primes(self, stop: int, first: int = 0, n: int = 0):
+        """The device sieving-prime table after prepare(stop): returns
+        (length, lo_excl, hi_incl, entries [first, first + n))."""
+        out = (ctypes.c_uint32 * max(n, 1))()
+        total, lo, hi = ctypes.c_size_t(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+        _check(self._lib.psg_sieving_primes(self._h, stop, first, out, n, ctypes.byref(total),
+                                            ctypes.byref(lo), ctypes.byref(hi)))
+        m = max(0, min(n, total.value - first))
+        return total.value, lo.value, hi.value, list(out[:m])
+
     def set_profiling(self, on: bool) -> None:
         _check(self._lib.psg_set_profiling(self._h, 1 if on else 0))
 
@@ -262,10 +284,11 @@ class Context:
     def reset_kernel_stats(self) -> None:
         _check(self._lib.psg_reset_kernel_stats(self._h))
 
-    def smem_atomic_rate(self) -> float:
-        v = ctypes.c_double(0)
-        _check(self._lib.psg_measure_smem_atomic_rate(self._h, ctypes.byref(v)))
-        return v.value
+    def smem_atomic_rates(self) -> Tuple[float, float]:
+        """(random-address, conflict-free) shared atomicAnd rates, atomics/s."""
+        r, c = ctypes.c_double(0), ctypes.c_double(0)
+        _check(self._lib.psg_measure_smem_atomic_rate(self._h, ctypes.byref(r), ctypes.byref(c)))
+        return r.value, c.value
 
     def bucket_entries(self, reset: bool = False) -> int:
         v = ctypes.c_uint64(0)
@@ -311,6 +334,11 @@ class Server:
         lat = (ctypes.c_double * max(n, 1))()
         _check(self._lib.psg_server_replay(self._h, arr, t, n, out, lat))
         return [list(out[6 * i:6 * i + 6]) for i in range(n)], list(lat[:n])
+
+    def inject_failure(self, nth: int, status: int) -> None:
+        """Tests: the nth request planned from now on fails its step with
+        `status` (psg_server_inject_failure)."""
+        _check(self._lib.psg_server_inject_failure(self._h, nth, status))
 
     def stats(self) -> dict:
         st = PsgServerStats()
@@ -386,6 +414,36 @@ def shard_of(start: int, stop: int, rank: int, world: int) -> Optional[Tuple[int
     if len(parts) < world:
         parts = parts + [None] * (world - len(parts))
     return parts[rank]
+
+
+def range_cost(start: int, stop: int) -> float:
+    """Estimated GPU work of counting [start, stop]: its crossings,
+    (8/30) * length * sum(1/p) over the sieving primes 59 < p <= sqrt(stop)
+    (~ ln ln sqrt(stop) - ln ln 59), plus a fixed per-range cost worth
+    1e7 integers (planning, launches, the last partial segment)."""
+    import math
+    if start > stop:
+        return 0.0
+    r = max(math.isqrt(stop), 61)
+    density = (8.0 / 30.0) * max(math.log(math.log(r)) - math.log(math.log(59.0)), 0.0)
+    return (stop - start + 1) * (density + 0.01) + 1e7 * 0.3
+
+
+def balance_ranges(ranges: Sequence[Tuple[int, int]], world: int) -> List[List[int]]:
+    """Indices of `ranges` ([(start, stop), ...]) per rank for a
+    one-process-per-GPU batch: longest-processing-time greedy on range_cost,
+    so that ranks get equal estimated work (lengths in a batch differ by
+    orders of magnitude; a split by index would not balance). Deterministic:
+    every rank computes the same split. Within a rank indices ascend."""
+    world = max(1, world)
+    order = sorted(range(len(ranges)), key=lambda i: (-range_cost(*ranges[i]), i))
+    load = [0.0] * world
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += range_cost(*ranges[i])
+    return [sorted(p) for p in parts]
 
 
 def count_sharded(count_fn, start: int, stop: int, kinds: int, rank: int, world: int,

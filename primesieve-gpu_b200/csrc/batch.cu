@@ -127,9 +127,9 @@ int Engine::launch_items(const BatchRange* d_ranges, const BatchItem* d_items, u
   b.num_items = n_items;
   b.queue = d_queue;
   b.counts = d_rows;
-  timed_begin(3, st);
+  timed_begin(2, st);
   cudaError_t e = launch_batch(b, st);
-  timed_end(3, st);
+  timed_end(2, st);
   if (e != cudaSuccess) { err = std::string("batch kernel launch: ") + cudaGetErrorString(e); return PSG_ERR_CUDA; }
   return PSG_OK;
 }

@@ -42,7 +42,6 @@ struct BucketArgs {
   const uint64_t* recip;
   const uint32_t* chunk_begin;  // [CTAs + 1] group-walk prime range per CTA
   const uint32_t* thread_chunk; // [CTAs + 1] thread-walk prime range per CTA
-  uint32_t list_base;         // list of CTA 0 (the sweep kernel's lists come first)
   uint32_t num_lists;         // lists per segment, all kernels
   const uint32_t* list_off;   // [num_lists] entry offset inside a segment region
   const uint32_t* list_cap;   // [num_lists] capacity
@@ -140,7 +139,7 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   if (tid < 3) s_round[tid] = 0;
   __syncthreads();
 
-  const uint32_t list = a.list_base + blockIdx.x;
+  const uint32_t list = blockIdx.x;
   const uint32_t cap = a.list_cap[list];
   uint32_t* const out = a.entries + a.list_off[list];
   const uint32_t win_bytes = W * a.seg_bytes;       // < 2^31 (host-checked)

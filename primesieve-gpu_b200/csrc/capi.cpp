@@ -49,8 +49,18 @@ psg::EngineConfig to_engine(const psg_config* c) {
   e.bucket_lists = c->bucket_lists;
   e.presieve = c->presieve;
   e.segments_per_launch = c->segments_per_launch;
-  e.sweep_limit = c->sweep_limit;
+  e.list_capacity_pct = c->list_capacity_pct;
   return e;
+}
+
+// Sets the message without throwing: a message that cannot be stored (no
+// host memory) leaves it empty.
+void fail_nothrow(const char* msg) noexcept {
+  try {
+    t_last_error = msg;
+  } catch (...) {
+    t_last_error.clear();
+  }
 }
 
 // Runs the body of a C entry point; no C++ exception (a failed host
@@ -61,11 +71,15 @@ int guarded(F&& body) {
   try {
     return body();
   } catch (const std::bad_alloc&) {
-    return fail(PSG_ERR_NOMEM, "out of host memory");
+    fail_nothrow("out of host memory");
+    return PSG_ERR_NOMEM;
   } catch (const std::exception& e) {
-    return fail(PSG_ERR_INTERNAL, std::string("internal error: ") + e.what());
+    fail_nothrow("internal error: ");
+    try { t_last_error += e.what(); } catch (...) {}
+    return PSG_ERR_INTERNAL;
   } catch (...) {
-    return fail(PSG_ERR_INTERNAL, "internal error: unknown exception");
+    fail_nothrow("internal error: unknown exception");
+    return PSG_ERR_INTERNAL;
   }
 }
 
@@ -74,6 +88,7 @@ int guarded(F&& body) {
 namespace psg {
 // Lets other translation units of the library report through psg_last_error().
 void set_last_error(const std::string& msg) { t_last_error = msg; }
+void set_last_error_nothrow(const char* msg) noexcept { fail_nothrow(msg); }
 }
 
 extern "C" {
@@ -146,6 +161,14 @@ int psg_server_get_stats(psg_server* s, psg_server_stats* out) {
   });
 }
 
+int psg_server_inject_failure(psg_server* s, uint32_t nth, int status) {
+  return guarded([&]() -> int {
+    if (!s || status == PSG_OK) return fail(PSG_ERR_ARG, "NULL server or status PSG_OK");
+    s->srv->inject_failure(nth, status);
+    return PSG_OK;
+  });
+}
+
 void psg_server_stop(psg_server* s) {
   if (!s) return;
   try {
@@ -170,6 +193,7 @@ const char* psg_status_string(int s) {
     case PSG_ERR_INTERNAL: return "internal error";
     case PSG_ERR_TIMEOUT: return "timed out";
     case PSG_ERR_CLOSED: return "closed";
+    case PSG_ERR_OVERFLOW: return "bucket list overflow in an asynchronous count";
     default: return "unknown status";
   }
 }
@@ -240,7 +264,7 @@ int psg_get_config(const psg_context* ctx, psg_config* out) {
     out->bucket_lists = c.bucket_lists;
     out->presieve = c.presieve;
     out->segments_per_launch = c.segments_per_launch;
-    out->sweep_limit = c.sweep_limit;
+    out->list_capacity_pct = c.list_capacity_pct;
     return PSG_OK;
   });
 }
@@ -271,6 +295,16 @@ int psg_count_async(psg_context* ctx, uint64_t start, uint64_t stop, uint32_t ki
     std::string err;
     int rc = ctx->engine.count_async(start, stop, kinds, reinterpret_cast<unsigned long long*>(dev_counts),
                                      static_cast<cudaStream_t>(stream), err);
+    return rc ? fail(rc, err) : PSG_OK;
+  });
+}
+
+int psg_count_async_status(psg_context* ctx) {
+  return guarded([&]() -> int {
+    if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    int rc = ctx->engine.async_status(err);
     return rc ? fail(rc, err) : PSG_OK;
   });
 }
@@ -351,6 +385,23 @@ int psg_prepare(psg_context* ctx, uint64_t stop) {
   });
 }
 
+int psg_sieving_primes(psg_context* ctx, uint64_t stop, size_t first, uint32_t* out, size_t n,
+                       size_t* total, uint64_t* lo_excl, uint64_t* hi_incl) {
+  return guarded([&]() -> int {
+    if (!ctx || !total || (n && !out)) return fail(PSG_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    std::string err;
+    size_t t = 0;
+    uint64_t lo = 0, hi = 0;
+    int rc = ctx->engine.sieving_primes(stop, first, out, n, t, lo, hi, err);
+    if (rc) return fail(rc, err);
+    *total = t;
+    if (lo_excl) *lo_excl = lo;
+    if (hi_incl) *hi_incl = hi;
+    return PSG_OK;
+  });
+}
+
 int psg_set_profiling(psg_context* ctx, int on) {
   return guarded([&]() -> int {
     if (!ctx) return fail(PSG_ERR_ARG, "NULL argument");
@@ -386,12 +437,15 @@ int psg_bucket_entries(psg_context* ctx, uint64_t* total, int reset) {
   });
 }
 
-int psg_measure_smem_atomic_rate(psg_context* ctx, double* atomics_per_s) {
+int psg_measure_smem_atomic_rate(psg_context* ctx, double* random_addr, double* conflict_free) {
   return guarded([&]() -> int {
-    if (!ctx || !atomics_per_s) return fail(PSG_ERR_ARG, "NULL argument");
+    if (!ctx || !random_addr) return fail(PSG_ERR_ARG, "NULL argument");
     std::lock_guard<std::mutex> lock(ctx->mu);
-    *atomics_per_s = ctx->engine.measure_smem_atomic_rate();
-    return *atomics_per_s > 0 ? PSG_OK : fail(PSG_ERR_CUDA, "probe kernel failed");
+    double r = 0, c = 0;
+    ctx->engine.measure_smem_atomic_rates(r, c);
+    *random_addr = r;
+    if (conflict_free) *conflict_free = c;
+    return (r > 0 && c > 0) ? PSG_OK : fail(PSG_ERR_CUDA, "probe kernel failed");
   });
 }
 

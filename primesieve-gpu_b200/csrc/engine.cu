@@ -2,7 +2,6 @@
 #include "engine.hpp"
 #include "sieve_kernel.cuh"
 #include "bucket_kernel.cuh"
-#include "sweep_kernel.cuh"
 #include "primegen_kernel.cuh"
 #include "../../include/psgpu.h"
 
@@ -45,8 +44,6 @@ constexpr double kSetupThread = 4.0;    // ... of a thread-walk prime
 constexpr double kTileFill = 0.4;
 constexpr double kFlushFill = 0.6;
 constexpr uint64_t kStaggerMultiples = 16;
-constexpr int kSweepWarps = 16;     // sweep CTA = 512 threads
-constexpr int kSweepK = 16;         // sieving primes per sweep lane
 
 #define PSG_CUDA(call)                                                          \
   do {                                                                          \
@@ -148,18 +145,29 @@ cudaError_t launch_sieve(uint32_t block, bool all, uint32_t grid, uint32_t smem,
   return cudaGetLastError();
 }
 
-// Roofline probe: random-address shared-memory atomicAnd throughput (the
-// operation the cross-off phase is made of). Each thread walks its own odd
-// word stride through a 32 KiB shared array; indices stay below kProbeWords.
+// Roofline probes of shared-memory atomicAnd, the operation the cross-off
+// phases are made of. RANDOM: each thread walks its own odd word stride, so
+// a warp's 32 addresses fall on banks at random (the access pattern of the
+// medium, direct and bucket phases). CONFLICT_FREE: lane l always hits a
+// word of bank l (word 32 k + l), one wavefront per warp instruction, the
+// device's shared-atomic ceiling. Indices stay below kProbeWords.
 constexpr uint32_t kProbeWords = 8192;    // 32 KiB of static shared memory
+template <bool CONFLICT_FREE>
 __global__ void __launch_bounds__(512) smem_atomic_probe_kernel(uint32_t iters, uint32_t* out) {
   __shared__ uint32_t s[kProbeWords];
   for (uint32_t i = threadIdx.x; i < kProbeWords; i += blockDim.x) s[i] = ~0u;
   __syncthreads();
   uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u;
   h ^= h >> 15; h *= 0x2c1b3c6du; h ^= h >> 12;
-  uint32_t w = h % kProbeWords;
-  const uint32_t stride = 2u * ((h >> 8) % 2048u) + 1u;     // < kProbeWords
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t w, stride;
+  if (CONFLICT_FREE) {
+    w = (threadIdx.x >> 5) * 32u * 7u % kProbeWords + lane;     // row of this warp, bank = lane
+    stride = 32u * 37u;                                         // whole rows: the bank stays
+  } else {
+    w = h % kProbeWords;
+    stride = 2u * ((h >> 8) % 2048u) + 1u;                      // < kProbeWords
+  }
   for (uint32_t it = 0; it < iters; it++) {
     atomicAnd(&s[w], ~(1u << (it & 31u)));
     w += stride;
@@ -169,27 +177,35 @@ __global__ void __launch_bounds__(512) smem_atomic_probe_kernel(uint32_t iters, 
   if (threadIdx.x == 0) out[blockIdx.x] = s[0];
 }
 
-} // namespace
-
-double Engine::measure_smem_atomic_rate() {
-  cudaSetDevice(device_);
-  const int grid = prop_.multiProcessorCount * 2;
-  uint32_t* out = nullptr;
-  if (cudaMalloc(&out, grid * sizeof(uint32_t)) != cudaSuccess) { cudaGetLastError(); return 0; }
+template <bool CONFLICT_FREE>
+double probe_rate(cudaStream_t st, int grid, uint32_t* out) {
   cudaEvent_t a, b;
   cudaEventCreate(&a); cudaEventCreate(&b);
-  smem_atomic_probe_kernel<<<grid, 512, 0, stream_>>>(64, out);
+  smem_atomic_probe_kernel<CONFLICT_FREE><<<grid, 512, 0, st>>>(64, out);
   const uint32_t iters = 8192;
-  cudaEventRecord(a, stream_);
-  smem_atomic_probe_kernel<<<grid, 512, 0, stream_>>>(iters, out);
-  cudaEventRecord(b, stream_);
+  cudaEventRecord(a, st);
+  smem_atomic_probe_kernel<CONFLICT_FREE><<<grid, 512, 0, st>>>(iters, out);
+  cudaEventRecord(b, st);
   cudaEventSynchronize(b);
   float ms = 0;
   cudaEventElapsedTime(&ms, a, b);
   cudaEventDestroy(a); cudaEventDestroy(b);
-  cudaFree(out);
   if (cudaGetLastError() != cudaSuccess || ms <= 0) return 0;
   return (double) grid * 512.0 * iters / (ms * 1e-3);
+}
+
+} // namespace
+
+void Engine::measure_smem_atomic_rates(double& random_rate, double& conflict_free_rate) {
+  random_rate = conflict_free_rate = 0;
+  cudaSetDevice(device_);
+  const int grid = prop_.multiProcessorCount * 2;
+  uint32_t* out = nullptr;
+  if (cudaMalloc(&out, grid * sizeof(uint32_t)) != cudaSuccess) { cudaGetLastError(); return; }
+  random_rate = probe_rate<false>(stream_, grid, out);
+  conflict_free_rate = probe_rate<true>(stream_, grid, out);
+  cudaStreamSynchronize(stream_);
+  cudaFree(out);
 }
 
 Engine::~Engine() {
@@ -215,9 +231,8 @@ Engine::~Engine() {
     if (g.h) cudaFreeHost(g.h);
     if (g.ev) cudaEventDestroy(g.ev);
   }
-  cudaFree(d_sweep_b_);
-  cudaFree(d_sweep_i_);
   cudaFree(d_overflow_);
+  cudaFree(d_async_overflow_);
   cudaFree(d_entry_total_);
   cudaFree(d_counts_);
   cudaFree(d_batch_rows_);
@@ -320,14 +335,14 @@ int Engine::init(int device, const EngineConfig& cfg, std::string& err) {
   allow_max_dynamic_smem(bucket_fill_kernel<kBucketBlock, true>, device_);
   allow_max_dynamic_smem(bucket_fill_kernel<kBucketBlock, false>, device_);
   allow_max_dynamic_smem(primegen_kernel<1024>, device_);
-  allow_max_dynamic_smem(bucket_sweep_kernel<32 * kSweepWarps, kSweepK>, device_);
-  // sweep primes need pdiv30 < 2^22 (state packing): p < 1.25e8
-  // (default: off -- the staged prime-major fill is faster on B200)
-  sweep_limit_ = std::min<uint32_t>(cfg.sweep_limit, 120000000u);
+  cap_scale_ = cfg.list_capacity_pct ? (double) cfg.list_capacity_pct / 100.0 : 1.0;
 
   PSG_CUDA(cudaMalloc(&d_counts_, 6 * sizeof(unsigned long long)));
   PSG_CUDA(cudaMalloc(&d_batch_queue_, sizeof(uint32_t)));
   PSG_CUDA(cudaMalloc(&d_overflow_, sizeof(uint32_t)));
+  PSG_CUDA(cudaMalloc(&d_async_overflow_, sizeof(uint32_t)));
+  PSG_CUDA(cudaMemset(d_async_overflow_, 0, sizeof(uint32_t)));
+  cur_overflow_ = d_overflow_;
   PSG_CUDA(cudaMalloc(&d_entry_total_, sizeof(unsigned long long)));
   PSG_CUDA(cudaMemset(d_entry_total_, 0, sizeof(unsigned long long)));
   PSG_CUDA(cudaMemset(d_overflow_, 0, sizeof(uint32_t)));
@@ -584,46 +599,41 @@ int Engine::prepare(uint64_t stop, std::string& err) {
   return ensure_primes(std::max<uint32_t>(isqrt_u64(stop), 7u), err);
 }
 
-// Bucket lists for the big primes primes[first, last):
-//  * sweep primes [first, mid): the segment-major sweep kernel, one list per
-//    sweep CTA; every CTA holds an interleaved share of the primes, so all
-//    sweep lists get the same capacity (the largest expected count + margin);
-//  * fill primes [mid, last): the prime-major kernel, one list per fill CTA,
-//    chunks cut for equal expected work (setup + hits per window).
-// Capacity = expected entries per segment + 6 sigma + 32 (x cap_scale_
-// after an overflow). All lists of one segment are packed in one region.
-int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::string& err) {
-  if (plan_.last && first == plan_.first && mid == plan_.mid && last == plan_.last && d_entries_) return PSG_OK;
+int Engine::sieving_primes(uint64_t stop, size_t first, uint32_t* out, size_t n, size_t& total,
+                           uint64_t& lo_excl, uint64_t& hi_incl, std::string& err) {
+  int rc = prepare(stop, err);
+  if (rc) return rc;
+  total = n_dev_;
+  lo_excl = presieve_max_;
+  hi_incl = primes_upto_;
+  if (first < n_dev_ && n) {
+    const size_t m = std::min(n, n_dev_ - first);
+    PSG_CUDA(cudaMemcpyAsync(out, d_primes_ + first, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    PSG_CUDA(cudaStreamSynchronize(stream_));
+  }
+  return PSG_OK;
+}
+
+// Bucket lists for the big primes primes[first, last): one list per fill
+// CTA and segment, the CTAs' prime chunks cut for equal expected work
+// (setup + hits per window). Capacity = expected entries per segment +
+// 6 sigma + 32 (x cap_scale_: grown after an overflow, or set below 1 by
+// the list_capacity_pct knob). All lists of one segment are packed in one
+// region.
+int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
+  if (plan_.last && first == plan_.first && last == plan_.last && d_entries_) return PSG_OK;
   const double span = (double) seg_bytes_ * 30.0;
   const double per_seg = span * (8.0 / 30.0);
   std::vector<uint32_t> off, cap, begin;
   uint64_t stride = 0;
   auto add_list = [&](double mu) {
     uint32_t ci = (uint32_t) std::ceil((mu + 6.0 * std::sqrt(mu) + 32.0) * cap_scale_);
-    ci = (ci + 3u) & ~3u;
+    ci = std::max<uint32_t>((ci + 3u) & ~3u, 4u);
     off.push_back((uint32_t) stride);
     cap.push_back(ci);
     stride += ci;
   };
-
-  // ---- sweep lists
-  const uint32_t nsweep = mid - first;
-  uint32_t sweep_ctas = 0;
-  if (nsweep) {
-    const uint32_t nw = (nsweep + 32u * kSweepK - 1) / (32u * kSweepK);
-    sweep_ctas = (nw + kSweepWarps - 1) / kSweepWarps;
-    const uint32_t nw_launch = sweep_ctas * kSweepWarps;
-    std::vector<double> mu(sweep_ctas, 0.0);
-    for (uint32_t idx = 0; idx < nsweep; idx++) {
-      const uint32_t gw = (idx / 32u) % nw_launch;
-      mu[gw / kSweepWarps] += per_seg / approx_prime(first + idx);
-    }
-    const double mu_max = *std::max_element(mu.begin(), mu.end());
-    for (uint32_t c = 0; c < sweep_ctas; c++) add_list(mu_max);
-  }
-
-  // ---- fill lists
-  const uint32_t nfill = last - mid;
+  const uint32_t nfill = last - first;
   uint32_t fill_ctas = 0;
   if (nfill) {
     fill_ctas = std::max<uint32_t>(1, std::min<uint32_t>(lists_, nfill));
@@ -632,11 +642,11 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
     // one in the thread walk
     // Per-window cost of a prime in entry units: its setup (8 lanes in the
     // group walk, one in the thread walk) plus its entries. Group walk:
-    // primes [mid, t_end); thread walk: primes [t_end, last). Each range is
+    // primes [first, t_end); thread walk: primes [t_end, last). Each range is
     // cut into fill_ctas chunks of equal cost (binary search on the monotone
     // cost over the 1/p prefix table); CTA c takes chunk c of both.
     const double setup_group = kSetupGroup, setup_thread = kSetupThread;
-    const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), mid), last);
+    const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), first), last);
     begin.assign(2 * (fill_ctas + 1), 0);
     const auto cut = [&](uint32_t from, uint32_t to, double setup, uint32_t* bounds) {
       const double s0 = inv_prefix(from);
@@ -654,7 +664,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
         bounds[l] = x;
       }
     };
-    cut(mid, t_end, setup_group, begin.data());
+    cut(first, t_end, setup_group, begin.data());
     uint32_t* tchunk = begin.data() + fill_ctas + 1;
     cut(t_end, last, setup_thread, tchunk);
     std::vector<double> mu(fill_ctas, 0.0);
@@ -663,14 +673,14 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
                          inv_prefix(tchunk[c + 1]) - inv_prefix(tchunk[c]));
     for (uint32_t c = 0; c < fill_ctas; c++) add_list(mu[c]);
   }
-  const uint32_t lists = sweep_ctas + fill_ctas;
+  const uint32_t lists = fill_ctas;
   if (stride > 0xffffffffull) { err = "bucket region too large"; return PSG_ERR_LIMIT; }
 
   const size_t need_entries = (size_t) stride * window_;
   const size_t need_counts = 2 * (size_t) lists * window_;   // counts, then spill counts
   // buffers grow only when no window can still be using them
   if (need_entries > entries_cap_ || need_counts > bcounts_cap_ || need_entries > entries2_cap_ ||
-      need_counts > bcounts2_cap_ || nsweep > sweep_state_cap_)
+      need_counts > bcounts2_cap_)
     quiesce();
   if (need_entries > entries_cap_) {
     cudaFree(d_entries_); d_entries_ = nullptr; entries_cap_ = 0;
@@ -701,24 +711,14 @@ int Engine::ensure_buckets(uint32_t first, uint32_t mid, uint32_t last, std::str
       d_entries2_ = nullptr; d_bcounts2_ = nullptr;
     }
   }
-  if (nsweep > sweep_state_cap_) {
-    cudaFree(d_sweep_b_); cudaFree(d_sweep_i_);
-    PSG_CUDA(cudaMalloc(&d_sweep_b_, (size_t) nsweep * sizeof(uint32_t)));
-    PSG_CUDA(cudaMalloc(&d_sweep_i_, (size_t) nsweep * sizeof(uint32_t)));
-    sweep_state_cap_ = nsweep;
-  }
   plan_.table.assign(off.begin(), off.end());
   plan_.table.insert(plan_.table.end(), cap.begin(), cap.end());
   if (fill_ctas) plan_.table.insert(plan_.table.end(), begin.begin(), begin.begin() + 2 * (fill_ctas + 1));
   plan_.first = first;
-  plan_.mid = mid;
   plan_.last = last;
   plan_.geom.seg_stride = stride;
   plan_.geom.lists = lists;
-  plan_.geom.sweep_ctas = sweep_ctas;
   plan_.geom.fill_ctas = fill_ctas;
-  plan_.geom.first = first;
-  plan_.geom.mid = mid;
   plan_gen_++;
   return PSG_OK;
 }
@@ -732,7 +732,7 @@ int Engine::plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err) {
   PlanSlot& sl = slots_[set];
   if (sl.gen == plan_gen_) return PSG_OK;
   const size_t n = plan_.table.size();
-  // sized once for any plan of lists_ fill lists (no sweep lists): growing
+  // sized once for any plan of lists_ fill lists: growing
   // waits for every window in flight
   const size_t want = std::max<size_t>(n, 4 * (size_t) lists_ + 8);
   if (n > sl.cap) {
@@ -876,8 +876,6 @@ int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err,
   // the rest go to buckets
   p.n_dir = std::max(p.n_med, std::min(below(big), p.n_total));
   p.buckets = p.n_dir < p.n_total;
-  // big primes below sweep_limit_: segment-major sweep; above: prime-major fill
-  p.n_sweep_end = std::max(p.n_dir, std::min(below(sweep_limit_), p.n_total));
   p.step = p.buckets ? window_ : (cfg_.segments_per_launch ? cfg_.segments_per_launch : p.nseg);
   return PSG_OK;
 }
@@ -900,7 +898,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   const bool use_buckets = p.buckets;
   int rc;
   if (use_buckets) {
-    rc = ensure_buckets(p.n_dir, p.n_sweep_end, p.n_total, err);
+    rc = ensure_buckets(p.n_dir, p.n_total, err);
     if (rc) return rc;
   }
 
@@ -919,10 +917,9 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   // Two or more bucket windows (or any in a chain): alternate windows on st
   // with list set 0 and on the auxiliary stream with set 1, so that the fill
   // of one window can use the SMs the other window's kernels leave idle at
-  // their tails. The segment-major sweep carries state from window to
-  // window: no overlap. While profiling, windows run one after another so
+  // their tails. While profiling, windows run one after another so
   // that each kernel's CUDA-event time is its own.
-  const bool two = use_buckets && !plan_.geom.sweep_ctas && d_entries2_ && aux_stream_ && !profiling_ &&
+  const bool two = use_buckets && d_entries2_ && aux_stream_ && !profiling_ &&
                    (chain_ || s_last - s_first > step);
   const bool fork = two && !chain_;
   if (!chain_) parity_ = 0;
@@ -946,38 +943,6 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
       const uint32_t* const t_off = slots_[set].d_table;      // [lists] list offsets
       const uint32_t* const t_cap = t_off + gm.lists;        // [lists] capacities
       const uint32_t* const t_chunk = t_cap + gm.lists;      // fill chunk bounds
-      if (gm.sweep_ctas) {
-        SweepArgs w;
-        std::memset(&w, 0, sizeof w);
-        w.win_low = win_low;
-        w.win_segments = (uint32_t) ns;
-        w.seg_bytes = seg_bytes_;
-        w.primes = d_primes_;
-        w.recip = d_recip_;
-        w.first = gm.first;
-        w.n = gm.mid - gm.first;
-        w.init = (s0 == 0) ? 1u : 0u;
-        w.state_b = d_sweep_b_;
-        w.state_i = d_sweep_i_;
-        w.list_base = 0;
-        w.num_lists_total = gm.lists;
-        w.list_off = t_off;
-        w.list_cap = t_cap;
-        w.seg_stride = gm.seg_stride;
-        w.entries = w_entries;
-        w.counts = w_counts;
-        w.overflow = d_overflow_;
-        w.entry_total = d_entry_total_;
-        for (uint32_t c = 0; c < 8; c++) {
-          w.wheel_tab[2 * c] = wheel_bits_packed(c);
-          w.wheel_tab[2 * c + 1] = wheel_corr_packed(c);
-        }
-        timed_begin(2, ws);
-        bucket_sweep_kernel<32 * kSweepWarps, kSweepK>
-            <<<gm.sweep_ctas, 32 * kSweepWarps, (size_t) ns * sizeof(uint32_t), ws>>>(w);
-        timed_end(2, ws);
-        PSG_CUDA(cudaGetLastError());
-      }
       if (gm.fill_ctas) {
         BucketArgs b;
         std::memset(&b, 0, sizeof b);
@@ -1001,7 +966,6 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.recip = d_recip_;
         b.chunk_begin = t_chunk;
         b.thread_chunk = t_chunk + gm.fill_ctas + 1;
-        b.list_base = gm.sweep_ctas;
         b.num_lists = gm.lists;
         b.list_off = t_off;
         b.list_cap = t_cap;
@@ -1009,7 +973,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.entries = w_entries;
         b.counts = w_counts;
         b.spill = w_counts + (size_t) gm.lists * window_;
-        b.overflow = d_overflow_;
+        b.overflow = cur_overflow_;
         b.entry_total = d_entry_total_;
         timed_begin(1, ws);
         if (seg_pow2_)
@@ -1022,7 +986,6 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
       a.bucket_entries = w_entries;
       a.bucket_counts = w_counts;
       a.bucket_spill = w_counts + (size_t) gm.lists * window_;
-      a.bucket_spill_base = gm.sweep_ctas;
       a.bucket_list_off = t_off;
       a.bucket_list_cap = t_cap;
       a.bucket_seg_stride = gm.seg_stride;
@@ -1045,18 +1008,45 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
   return PSG_OK;
 }
 
-int Engine::count_async(uint64_t start, uint64_t stop, uint32_t kinds,
-                        unsigned long long* dev_counts, cudaStream_t stream, std::string& err) {
+int Engine::count_ordered(uint64_t start, uint64_t stop, uint32_t kinds, unsigned long long* dev_counts,
+                          cudaStream_t stream, uint32_t* flag, std::string& err) {
   PSG_CUDA(cudaSetDevice(device_));
   cudaStream_t st = stream ? stream : stream_;
-  // The engine's scratch (bucket lists, sweep state) is shared by all counts
-  // of this context: order this count after the previous one, whatever
-  // stream that one ran on.
+  // The engine's scratch (bucket lists) is shared by all counts of this
+  // context: order this count after the previous one, whatever stream that
+  // one ran on.
   if (last_stream_ && last_stream_ != st) PSG_CUDA(cudaStreamWaitEvent(st, done_event_, 0));
+  cur_overflow_ = flag;
   int rc = count_enqueue(start, stop, kinds, dev_counts, st, err);
+  cur_overflow_ = d_overflow_;
   PSG_CUDA(cudaEventRecord(done_event_, st));
   last_stream_ = st;
   return rc;
+}
+
+// Asynchronous counts cannot recount on an overflow; their fill kernels
+// raise a flag of their own, which only async_status reads and clears, so
+// no synchronous path's reset of d_overflow_ can hide it.
+int Engine::count_async(uint64_t start, uint64_t stop, uint32_t kinds,
+                        unsigned long long* dev_counts, cudaStream_t stream, std::string& err) {
+  async_pending_ = true;
+  return count_ordered(start, stop, kinds, dev_counts, stream, d_async_overflow_, err);
+}
+
+int Engine::async_status(std::string& err) {
+  PSG_CUDA(cudaSetDevice(device_));
+  if (!async_pending_) return PSG_OK;
+  PSG_CUDA(cudaEventSynchronize(done_event_));
+  PSG_CUDA(cudaMemcpyAsync(h_counts_ + 7, d_async_overflow_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+  PSG_CUDA(cudaMemsetAsync(d_async_overflow_, 0, sizeof(uint32_t), stream_));
+  PSG_CUDA(cudaStreamSynchronize(stream_));
+  async_pending_ = false;
+  if ((uint32_t) (h_counts_[7] & 0xffffffffu)) {
+    grow_bucket_lists();
+    err = "a bucket list overflowed during an asynchronous count: its counts are too high; count again";
+    return PSG_ERR_OVERFLOW;
+  }
+  return PSG_OK;
 }
 
 int Engine::count_enqueue(uint64_t start, uint64_t stop, uint32_t kinds,
@@ -1082,7 +1072,7 @@ int Engine::count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts
   for (int attempt = 0; attempt < 4; attempt++) {
     PSG_CUDA(cudaMemsetAsync(d_counts_, 0, 6 * sizeof(unsigned long long), stream_));
     PSG_CUDA(cudaMemsetAsync(d_overflow_, 0, sizeof(uint32_t), stream_));
-    int rc = count_async(start, stop, kinds, d_counts_, stream_, err);
+    int rc = count_ordered(start, stop, kinds, d_counts_, stream_, d_overflow_, err);
     if (rc) return rc;
     PSG_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
     PSG_CUDA(cudaMemcpyAsync(h_counts_ + 6, d_overflow_, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));

@@ -26,7 +26,7 @@ struct EngineConfig {
   uint32_t bucket_lists = 0;     // lists (bucket CTAs) per segment; 0 = auto
   uint32_t presieve = 0;         // pre-sieve tables: 0 = default (on), 1 = on, 2 = off
   uint32_t segments_per_launch = 0; // cap on segments per sieve launch; 0 = auto
-  uint32_t sweep_limit = 0;      // big primes below: segment-major sweep; 0 = auto
+  uint32_t list_capacity_pct = 0; // bucket-list capacity, % of the estimate (0 = 100)
 };
 
 // One range of a batch; same layout as psg_range (include/psgpu.h).
@@ -68,11 +68,11 @@ constexpr uint32_t kThreadWalkDiv = 32;
 
 // Prime tiers and launch geometry of one range [lo, hi] (lo >= 7):
 // primes [0, n_small) warp-cooperative, [n_small, n_med) carried state,
-// [n_med, n_dir) direct, [n_dir, n_total) bucket lists (sweep below
-// n_sweep_end); sieve launches of `step` segments.
+// [n_med, n_dir) direct, [n_dir, n_total) bucket lists; sieve launches of
+// `step` segments.
 struct RangePlan {
   uint64_t lo = 0, hi = 0, seg_low0 = 0, nseg = 0, step = 1;
-  uint32_t n_small = 0, n_med = 0, n_dir = 0, n_sweep_end = 0, n_total = 0;
+  uint32_t n_small = 0, n_med = 0, n_dir = 0, n_total = 0;
   bool buckets = false;
   uint64_t windows() const { return (nseg + step - 1) / step; }
 };
@@ -98,6 +98,11 @@ public:
   // (nullptr: the engine's stream). No host synchronisation.
   int count_async(uint64_t start, uint64_t stop, uint32_t kinds,
                   unsigned long long* dev_counts, cudaStream_t stream, std::string& err);
+
+  // Waits for every count issued so far; PSG_ERR_OVERFLOW if a bucket list
+  // of a count_async since the last call overflowed (entries dropped: those
+  // counts are too high), after growing the lists. Clears the record.
+  int async_status(std::string& err);
 
   // Synchronous host-result version (counts[6] overwritten).
   int count(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t counts[6], std::string& err);
@@ -156,6 +161,11 @@ public:
 
   // Make sure the sieving-prime table covers sqrt(stop) (host work + upload).
   int prepare(uint64_t stop, std::string& err);
+  // prepare(stop), then entries [first, first + n) of the device table (clipped)
+  // into host out; total = its length, and it holds the primes p with
+  // lo_excl < p <= hi_incl.
+  int sieving_primes(uint64_t stop, size_t first, uint32_t* out, size_t n, size_t& total,
+                     uint64_t& lo_excl, uint64_t& hi_incl, std::string& err);
 
   int device() const { return device_; }
   const cudaDeviceProp& props() const { return prop_; }
@@ -176,9 +186,11 @@ public:
   // Bucket entries written since the last reset (device counter; syncs).
   uint64_t bucket_entries();
   void reset_bucket_entries();
-  // Measured random-address shared-memory atomicAnd rate (atomics/s), the
-  // roofline denominator of the cross-off phase.
-  double measure_smem_atomic_rate();
+  // Measured shared-memory atomicAnd rates (atomics/s), the roofline
+  // denominators of the cross-off phases: random addresses (bank conflicts
+  // as in the medium, direct and bucket phases) and conflict-free (every
+  // lane on its own bank: the ceiling).
+  void measure_smem_atomic_rates(double& random_rate, double& conflict_free_rate);
 
 private:
   int build_presieve(std::string& err);
@@ -195,7 +207,7 @@ private:
   // in a window of w segments: the fill kernel walks them one lane per prime
   // (one first-multiple setup instead of eight)
   uint64_t thread_limit(uint32_t w) const { return (uint64_t) w * seg_bytes_ / kThreadWalkDiv; }
-  int ensure_buckets(uint32_t first_big, uint32_t mid_big, uint32_t last_big, std::string& err);
+  int ensure_buckets(uint32_t first_big, uint32_t last_big, std::string& err);
   int plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err);
   void quiesce();
   int run(uint64_t lo, uint64_t hi, uint32_t kinds, unsigned long long* dev_counts,
@@ -205,6 +217,10 @@ private:
   uint64_t count_range(uint64_t lo, uint64_t hi, std::string& err, int& rc);
   int count_enqueue(uint64_t start, uint64_t stop, uint32_t kinds,
                     unsigned long long* dev_counts, cudaStream_t st, std::string& err);
+  // count_enqueue after everything issued before, on stream (nullptr: the
+  // engine's stream); its fill kernels report overflow to `flag`
+  int count_ordered(uint64_t start, uint64_t stop, uint32_t kinds, unsigned long long* dev_counts,
+                    cudaStream_t stream, uint32_t* flag, std::string& err);
   void timed_begin(int which, cudaStream_t st);
   void timed_end(int which, cudaStream_t st);
 
@@ -255,10 +271,10 @@ private:
   // fill chunk bounds]; gen changes with every new plan.
   struct PlanGeom {
     uint64_t seg_stride = 0;              // entries per segment region
-    uint32_t lists = 0, sweep_ctas = 0, fill_ctas = 0, first = 0, mid = 0;
+    uint32_t lists = 0, fill_ctas = 0;
   };
   struct BucketPlan {
-    uint32_t first = 0, mid = 0, last = 0;   // last == 0: none
+    uint32_t first = 0, last = 0;            // last == 0: none
     PlanGeom geom;
     std::vector<uint32_t> table;
   };
@@ -285,12 +301,11 @@ private:
   bool chain_ = false;                     // window sets alternate across run_windows calls
   bool batch_smem_set_ = false;            // persistent kernel's shared-memory limit raised
   uint32_t parity_ = 0;                    // next window's list set (bit 0)
-  uint32_t sweep_limit_ = 0;
-  uint32_t* d_sweep_b_ = nullptr;
-  uint32_t* d_sweep_i_ = nullptr;
-  size_t sweep_state_cap_ = 0;
   double cap_scale_ = 1.0;
-  uint32_t* d_overflow_ = nullptr;
+  uint32_t* d_overflow_ = nullptr;         // overflow flag of synchronous paths (reset per use)
+  uint32_t* d_async_overflow_ = nullptr;   // sticky flag of count_async, read by async_status
+  uint32_t* cur_overflow_ = nullptr;       // the flag the next fill launches report to
+  bool async_pending_ = false;             // count_async issued since the last async_status
   unsigned long long* d_entry_total_ = nullptr;
   uint64_t overflow_retries_ = 0;
 
@@ -314,8 +329,8 @@ private:
   bool profiling_ = false;
   // launches are always counted; CUDA-event times only while profiling
   struct Timed { const char* name; std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev; uint64_t launches = 0; double ms = 0; };
-  Timed timed_[4] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 },
-                      { "bucket_sweep_kernel", {}, 0, 0 }, { "batch_sieve_kernel", {}, 0, 0 } };
+  Timed timed_[3] = { { "sieve_count_kernel", {}, 0, 0 }, { "bucket_fill_kernel", {}, 0, 0 },
+                      { "batch_sieve_kernel", {}, 0, 0 } };
 };
 
 } // namespace psg

@@ -1,10 +1,11 @@
 // noalloc.cu -- psg_count_noalloc(): counting without any allocation.
 //
 // Some callers cannot allocate device memory at the moment they count:
-// code running while a CUDA graph is being captured (cudaMalloc is not
-// allowed then), allocators' own callbacks, real-time loops that must not
-// touch the allocator, or embedders that give a library a fixed memory
-// budget. For them this entry point runs the same segment-sieve kernel as
+// allocators' own callbacks (a cudaMalloc there re-enters the allocator),
+// real-time loops that must not touch the allocator (a cudaMalloc can
+// synchronise the device and take milliseconds), or embedders that give a
+// library a fixed memory budget and account for every byte of it. For them
+// this entry point runs the same segment-sieve kernel as
 // psg_count(), but every piece of scratch it needs -- the sieving-prime
 // table, its reciprocals and the six count accumulators -- lives in one
 // file-scope static __device__ array of fixed size (kScratchBytes, about
@@ -25,9 +26,13 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 
-namespace psg { void set_last_error(const std::string& msg); }   // capi.cpp
+namespace psg {                                                   // capi.cpp
+void set_last_error(const std::string& msg);
+void set_last_error_nothrow(const char* msg) noexcept;
+}
 
 namespace {
 
@@ -130,10 +135,7 @@ int setup_device(int dev, DeviceSetup& d) {
   return PSG_OK;
 }
 
-} // namespace
-
-extern "C" int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
-                                 uint64_t* dev_counts, void* stream) {
+int count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds, uint64_t* dev_counts, void* stream) {
   if (!dev_counts) return fail(PSG_ERR_ARG, "psg_count_noalloc: dev_counts is NULL");
   if (stop > kMaxStop)
     return fail(PSG_ERR_LIMIT, "psg_count_noalloc: stop must be <= 2^36 = 68719476736 (its sieving "
@@ -208,4 +210,22 @@ extern "C" int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(PSG_ERR_CUDA, std::string("finish kernel launch: ") + cudaGetErrorString(e));
   return PSG_OK;
+}
+
+} // namespace
+
+// No C++ exception may unwind through the C boundary: a message that
+// cannot be built (no host memory) or a mutex that cannot be taken becomes
+// a status, as for every other psg_* entry point.
+extern "C" int psg_count_noalloc(uint64_t start, uint64_t stop, uint32_t kinds,
+                                 uint64_t* dev_counts, void* stream) {
+  try {
+    return count_noalloc(start, stop, kinds, dev_counts, stream);
+  } catch (const std::bad_alloc&) {
+    psg::set_last_error_nothrow("psg_count_noalloc: out of host memory");
+    return PSG_ERR_NOMEM;
+  } catch (...) {
+    psg::set_last_error_nothrow("psg_count_noalloc: internal error");
+    return PSG_ERR_INTERNAL;
+  }
 }

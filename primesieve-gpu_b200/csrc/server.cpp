@@ -195,6 +195,12 @@ int Server::replay(const RangeQuery* q, const double* arrival_s, size_t n, uint6
   return rc;
 }
 
+void Server::inject_failure(uint32_t nth, int status) {
+  std::lock_guard<std::mutex> lk(mu_);
+  inject_countdown_ = nth;
+  inject_status_ = status;
+}
+
 ServerStats Server::stats() {
   std::lock_guard<std::mutex> lk(mu_);
   return stats_;
@@ -230,6 +236,8 @@ void Server::loop() {
         for (Request* r : left) finish(r, PSG_ERR_CLOSED, "server stopped");
         return;
       }
+      // free_slots_ and active_ belong to the worker thread (start() fills
+      // free_slots_ before the worker exists); mu_ guards only pending_ here
       while (!pending_.empty() && !free_slots_.empty()) {
         Request* r = pending_.front();
         pending_.pop_front();
@@ -247,7 +255,11 @@ void Server::loop() {
       stats_.gpu_busy_seconds += std::chrono::duration<double>(Clock::now() - t).count();
     }
     if (rc) {
-      // a failed step leaves the rows unreliable: fail what is in flight
+      // a failed step leaves the rows unreliable: fail what is in flight,
+      // and the requests admitted in this step that it did not get to plan
+      // (refused ones are already finished and nulled out of `admitted`)
+      for (Request* r : admitted)
+        if (r && !r->planned) { free_slots_.push_back(r->slot); finish(r, rc, err); }
       for (Request* r : active_) { free_slots_.push_back(r->slot); finish(r, rc, err); }
       active_.clear();
     }
@@ -259,7 +271,14 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
   SRV_CUDA(cudaSetDevice(eng_.device()));
 
   // ---- plan the newly admitted requests
-  for (Request* r : admitted) {
+  for (Request*& r : admitted) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (inject_countdown_ && --inject_countdown_ == 0) {
+        err = "injected failure (psg_server_inject_failure)";
+        return inject_status_;
+      }
+    }
     const uint64_t lo = std::max<uint64_t>(r->start, 7), hi = r->stop;
     // batch class unless the range needs the bucket path, or its segments
     // are so costly (many direct-tier primes, each located again per
@@ -281,7 +300,9 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
       }
       if (rc) {
         free_slots_.push_back(r->slot);
-        finish(r, rc, err);
+        Request* done = r;
+        r = nullptr;                 // a waiter may free it once it is finished
+        finish(done, rc, err);
         err.clear();
         continue;
       }

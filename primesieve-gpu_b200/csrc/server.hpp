@@ -62,6 +62,10 @@ public:
   int replay(const RangeQuery* q, const double* arrival_s, size_t n, uint64_t* counts,
              double* latency_s, std::string& err);
   ServerStats stats();
+  // Tests of the failure handling: the nth request planned from now on
+  // (nth >= 1; 0 cancels) makes its step fail with `status` at that point,
+  // as a failed CUDA call there would.
+  void inject_failure(uint32_t nth, int status);
 
 private:
   using Clock = std::chrono::steady_clock;
@@ -102,6 +106,8 @@ private:
   std::deque<Request*> pending_;
   std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs_;
   ServerStats stats_;
+  uint32_t inject_countdown_ = 0;   // guarded by mu_
+  int inject_status_ = 0;
 
   // worker-only
   std::vector<Request*> active_;

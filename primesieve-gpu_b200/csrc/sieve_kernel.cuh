@@ -78,10 +78,8 @@ struct SieveArgs {
   const uint32_t* bucket_entries;   // [segment][seg_stride] entries
   const uint32_t* bucket_counts;    // [segment][list] entries from the list's start
   const uint32_t* bucket_spill;     // [segment][list] entries at the list's top
-                                    // (lists >= bucket_spill_base only)
   const uint32_t* bucket_list_off;  // [list] offset inside a segment region
   const uint32_t* bucket_list_cap;  // [list] capacity
-  uint32_t bucket_spill_base;       // first list with a spill region
   uint64_t bucket_seg_stride;       // entries per segment region
   uint32_t num_bucket_lists;        // lists per segment (0: no big primes)
   uint32_t wheel_tab[16];           // per class: bits, corr (wheel walk)
@@ -506,10 +504,9 @@ __device__ __forceinline__ void phase_buckets(const SieveArgs& a, uint64_t s, ui
     l = __shfl_sync(0xffffffffu, l, 0);
     if (l >= a.num_bucket_lists) break;
     // the list's length, spill count and place, loaded together
-    const bool has_spill = l >= a.bucket_spill_base;
     const uint32_t n = __ldg(cnt + l);
-    const uint32_t ns = has_spill ? __ldg(spill + l) : 0u;
-    const uint32_t cap = has_spill ? __ldg(a.bucket_list_cap + l) : 0u;
+    const uint32_t ns = __ldg(spill + l);
+    const uint32_t cap = __ldg(a.bucket_list_cap + l);
     const uint32_t* e = seg_entries + __ldg(a.bucket_list_off + l);
     const uint32_t n4 = n & ~3u;
     // four 16-byte loads in flight per lane before the atomics that use them

@@ -16,7 +16,7 @@ committed JSON).
    oracle/Makefile.ref) for the case list of test/gpu_count.cpp:86-113, the
    sizes the benchmark runs, edge ranges near 2^64 and seeded random ranges.
 
-Usage: python tests/golden/make_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_golden.py --ref <reference source tree>
 """
 import argparse
 import ctypes
@@ -180,7 +180,7 @@ BENCH_CASES = [
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference source tree")
     ap.add_argument("--lib", default=os.path.join(REPO, "oracle", "_ref", "libprimesieve_ref.so"))
     ap.add_argument("--skip-bench", action="store_true")
     args = ap.parse_args()

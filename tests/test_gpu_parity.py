@@ -65,8 +65,8 @@ CONFIGS = [
     dict(seg_bytes=16384, block=256, small_limit=100000),   # only warp-cooperative
     dict(seg_bytes=4096, block=256, big_limit=200, window_segments=3, bucket_lists=5),
     dict(seg_bytes=65536, block=1024, big_limit=1000, window_segments=7),
-    dict(seg_bytes=4096, block=256, big_limit=300, sweep_limit=3000, window_segments=5),   # sweep + fill
-    dict(seg_bytes=16384, block=512, big_limit=500, sweep_limit=500, bucket_lists=3),      # fill only
+    dict(seg_bytes=4096, block=256, big_limit=300, window_segments=5),                     # many short windows
+    dict(seg_bytes=16384, block=512, big_limit=500, bucket_lists=3),                       # few lists
     dict(seg_bytes=32768, block=512, ctas_per_sm=2),
     # segment size not a power of two: the fill's segment index by reciprocal
     dict(seg_bytes=12288, block=256, big_limit=300, window_segments=9),
@@ -168,6 +168,71 @@ def test_count_async_first_call_exact(psg, a, b, k):
     assert got == want
     if (a, k) == (10 ** 15, 1):
         assert got[0] == 2895317534               # reference CPU library
+
+
+def test_count_async_overflow_is_reported(psg):
+    """With lists at a quarter of their estimated capacity the bucket fill
+    drops entries. psg_count_async cannot recount, so psg_count_async_status
+    must report PSG_ERR_OVERFLOW (9) -- also after a synchronous count on the
+    same context, which resets only its own flag -- and, once the lists have
+    grown, an asynchronous count is exact again and reports PSG_OK."""
+    import torch
+    a, b = 10 ** 15, 10 ** 15 + 10 ** 10
+    stream = torch.cuda.current_stream().cuda_stream
+    with psg.Context(list_capacity_pct=25) as c:
+        dev = torch.zeros(6, dtype=torch.int64, device="cuda")
+        c.count_async(a, b, 1, dev.data_ptr(), stream)
+        want = c.count(a, b, 1)                  # recounts internally: exact
+        with pytest.raises(psg.PsgError) as e:
+            c.count_async_status()
+        assert e.value.status == 9 and "overflow" in str(e.value)
+        c.count_async_status()                   # the record was cleared
+        for attempt in range(4):
+            dev.zero_()
+            c.count_async(a, b, 1, dev.data_ptr(), stream)
+            try:
+                c.count_async_status()
+                break
+            except psg.PsgError as err:
+                assert err.status == 9
+        else:
+            pytest.fail("lists did not grow")
+        torch.cuda.synchronize()
+        assert dev.tolist() == want
+    assert want[0] == 289531946                  # oracle: pi[1e15, 1e15+1e10]
+
+
+def test_count_recounts_on_overflow(psg, ctx):
+    """The synchronous path detects the overflow and recounts with grown
+    lists: exact however small the lists start."""
+    cases = [(10 ** 15, 10 ** 15 + 10 ** 10, 1), (2 ** 64 - 2 ** 33, 2 ** 64 - 1, 63)]
+    with psg.Context(list_capacity_pct=20) as c:
+        for a, b, k in cases:
+            assert c.count(a, b, k) == ctx.count(a, b, k), (a, b, k)
+        assert c.count_batch([(a, b, k) for a, b, k in cases]) == [ctx.count(a, b, k) for a, b, k in cases]
+
+
+def test_device_prime_table(psg, oracle):
+    """The sieving-prime table generated on the device up to 2^32: its
+    length (the primes 59 < p < 2^32: pi(2^32) = 203280221 less the 17 primes
+    <= 59), its first and last entries, its index at 1e9 (pi(1e9) =
+    50847534) and seeded windows, against the oracle's primes."""
+    with psg.Context() as c:
+        top = 2 ** 64 - 1
+        total, lo, hi, head = c.sieving_primes(top, 0, 2000)
+        assert (lo, hi) == (59, 2 ** 32 - 1)
+        assert total == 203280221 - 17
+        assert head == oracle.primes(60, head[-1]) and len(head) == 2000
+        _, _, _, tail = c.sieving_primes(top, total - 500, 1000)
+        assert len(tail) == 500 and tail[-1] == 4294967291
+        assert tail == oracle.primes(tail[0], 2 ** 32 - 1)
+        _, _, _, at = c.sieving_primes(top, 50847534 - 17 - 1, 2)
+        assert at == [999999937, 1000000007]
+        rng = random.Random(7)
+        for _ in range(12):
+            i = rng.randrange(total - 20000)
+            _, _, _, win = c.sieving_primes(top, i, 20000)
+            assert win == oracle.primes(win[0], win[-1]), i
 
 
 def test_c_api(psg, ctx):

@@ -101,3 +101,33 @@ def test_closing_the_context_stops_its_server(psg):
     with pytest.raises(psg.PsgError) as e:
         srv.submit(0, 100, 1)      # stopped: a NULL server handle
     assert e.value.status == 1
+
+
+def test_failed_step_leaves_no_waiter_blocked(psg, ctx):
+    """A step that fails while planning its admitted requests (injected on the
+    host: the second request planned makes its step fail with
+    PSG_ERR_CUDA, 3) completes every request of that step -- the ones it had
+    planned and the ones it had not reached -- with the error, and the
+    server goes on serving."""
+    import threading
+    reqs = [(10 ** 12 + i * 10 ** 7, 10 ** 12 + (i + 1) * 10 ** 7, 1) for i in range(8)]
+    with psg.Server(ctx) as srv:
+        srv.inject_failure(2, 3)
+        out = [None] * len(reqs)
+
+        def run():
+            try:
+                out[:] = srv.replay(reqs, [0.0] * len(reqs))[0]
+            except psg.PsgError as e:
+                out[:] = [e.status] * len(reqs)
+
+        t = threading.Thread(target=run, daemon=True)
+        t.start()
+        t.join(timeout=120)
+        assert not t.is_alive(), "a waiter stayed blocked after the failed step"
+        assert out[0] == 3                   # replay reports the first failure
+        st = srv.stats()
+        assert st["completed"] + st["refused"] == st["submitted"] == len(reqs)
+        assert st["refused"] >= 1
+        rid = srv.submit(*reqs[0])
+        assert srv.wait(rid)[0] == ctx.count(*reqs[0])

@@ -1,6 +1,7 @@
 """GPU: psg_count_noalloc(), the entry point for callers that cannot
-allocate device memory while they count (code inside CUDA graph capture,
-allocator callbacks, real-time loops, fixed-budget embedders). It keeps all
+allocate device memory while they count (an allocator's own callbacks,
+real-time loops where a cudaMalloc could synchronise the device, embedders
+with a fixed memory budget). It keeps all
 of its scratch in one fixed static device array, so these tests check that
 back-to-back calls (which reuse that array) give exactly what psg_count()
 gives, and that a stop beyond its limit is refused with a clear error.
