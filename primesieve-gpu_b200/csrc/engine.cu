@@ -524,7 +524,12 @@ int Engine::ensure_primes(uint64_t limit, std::string& err) {
   }
   // prefix of sum(1/p) per sample block: exact inside the host head, the
   // block's first (smallest) prime for all of a block beyond it (an upper
-  // bound, which is what the bucket capacities need)
+  // bound, which is what the bucket capacities need); per prime inside the
+  // head
+  if (h_inv_head_.size() != h_primes_.size() + 1) {
+    h_inv_head_.assign(h_primes_.size() + 1, 0.0);
+    for (size_t j = 0; j < h_primes_.size(); j++) h_inv_head_[j + 1] = h_inv_head_[j] + 1.0 / (double) h_primes_[j];
+  }
   h_inv_block_.assign(ns + 1, 0.0);
   for (size_t k = 0; k < ns; k++) {
     const size_t j0 = k * kSample, j1 = std::min<size_t>(j0 + kSample, n_dev_);
@@ -586,11 +591,18 @@ double Engine::approx_prime(uint32_t i) const {
 }
 
 // Sum of 1/p over table primes [0, i), same weights as h_inv_block_.
+// O(1): the bucket planner's binary searches call it thousands of times per
+// range.
 double Engine::inv_prefix(uint32_t i) const {
-  const size_t k = i / kSample;
-  double v = h_inv_block_[std::min(k, h_inv_block_.size() - 1)];
-  for (size_t j = k * kSample; j < i; j++)
-    v += 1.0 / (double) (j < h_primes_.size() ? h_primes_[j] : h_sample_[k]);
+  const size_t head = h_primes_.size();
+  if (i <= head) return h_inv_head_[i];
+  const size_t k = std::min<size_t>(i / kSample, h_inv_block_.size() - 1);
+  const size_t j0 = k * kSample;
+  double v = h_inv_block_[k];
+  // [j0, i): exact inside the head, the block's smallest prime beyond it
+  const size_t jh = std::min<size_t>(std::max(j0, head), i);
+  if (jh > j0) v += h_inv_head_[jh] - h_inv_head_[j0];
+  if (i > jh) v += (double) (i - jh) / (double) h_sample_[std::min(k, h_sample_.size() - 1)];
   return v;
 }
 

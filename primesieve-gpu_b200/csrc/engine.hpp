@@ -250,6 +250,7 @@ private:
   std::vector<uint32_t> h_primes_;
   std::vector<uint32_t> h_sample_;
   std::vector<double> h_inv_block_;      // [blocks + 1] prefix of sum(1/p) per sample block
+  std::vector<double> h_inv_head_;       // [head + 1] prefix of sum(1/p) over the exact head
   size_t n_dev_ = 0;
   uint64_t primes_upto_ = 0;
   uint32_t* d_primes_ = nullptr;
