@@ -28,7 +28,7 @@ configs  : pi(1e9), the six counts of [0, 1e11] and of [2^64-2^34, 2^64-1],
            reference CLI's time on the full range in the same run;
 serving  : the seed-1 request stream (lengths 2^12..2^36, starts up to
            1.8e19, kinds 1..6) replayed through psg_server_replay at
-           100 .. 50k requests/s: p50/p99 latency and integers/s per rate,
+           100, 300, 1k, 3k, 10k and 50k requests/s: p50/p99 latency and integers/s per rate,
            beside the reference library replaying a seeded sample of it;
 batched  : the 4096-range workload through psg_count_batch vs one psg_count
            per range, beside the reference library on a sample of it.
@@ -530,7 +530,7 @@ def serving_section(psg, ctx, args):
     import random
     import numpy as np
     n = args.serving_requests
-    rates = [100.0, 1000.0, 10000.0, 50000.0]
+    rates = [100.0, 300.0, 1000.0, 3000.0, 10000.0, 50000.0]
     rows = []
     ok = True
     with psg.Server(ctx) as srv:
@@ -663,6 +663,7 @@ def batch_section(psg, ctx, rank, world, args, torch, dist):
         "autotune": {"seconds": round(t_tune, 2),
                      "classes": [{"digits": r["range_class"] + 1, "direct_budget": r["direct_budget"],
                                   "big_limit": r["big_limit"], "stripe": r["stripe"],
+                                  "small_limit": r["small_limit"],
                                   "sample_s": round(r["best_seconds"], 4), "default_s": round(r["default_seconds"], 4)}
                                  for r in tuned]},
     }

@@ -163,8 +163,9 @@ int psg_nth_prime(psg_context* ctx, int64_t n, uint64_t start, uint64_t* prime);
 /* Batch autotuner (no reference counterpart). Range classes are the decimal
  * lengths of stop; for every class present in `ranges` a seeded sample of
  * its ranges is counted under candidate parameters -- the batch-kernel vs
- * bucket-path budget, the direct-tier extent of bucket-path ranges and the
- * stripe length of work items -- and the fastest are kept in the context for
+ * bucket-path budget, the direct-tier extent of bucket-path ranges, the
+ * stripe length of work items, then the small/medium sieving-prime
+ * threshold -- and the fastest are kept in the context for
  * psg_count_batch and the server. Stops after about budget_seconds. One
  * report row per tuned class (up to cap rows; *count = rows). */
 typedef struct {
@@ -176,6 +177,8 @@ typedef struct {
   uint32_t stripe;             /* chosen: segments per work item */
   double best_seconds;         /* sample time with the chosen parameters */
   double default_seconds;      /* sample time with the defaults */
+  uint32_t small_limit;        /* chosen: warp-cooperative tier below this prime (0: default) */
+  uint32_t reserved;
 } psg_tune_class;
 
 int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, double budget_seconds,

@@ -59,7 +59,8 @@ class PsgTuneClass(ctypes.Structure):
     _fields_ = [("range_class", ctypes.c_int32), ("sample_ranges", ctypes.c_uint32),
                 ("sample_integers", ctypes.c_double), ("direct_budget", ctypes.c_double),
                 ("big_limit", ctypes.c_uint32), ("stripe", ctypes.c_uint32),
-                ("best_seconds", ctypes.c_double), ("default_seconds", ctypes.c_double)]
+                ("best_seconds", ctypes.c_double), ("default_seconds", ctypes.c_double),
+                ("small_limit", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class PsgServerConfig(ctypes.Structure):

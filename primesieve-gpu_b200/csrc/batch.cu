@@ -62,7 +62,8 @@ uint64_t Engine::range_segments(const BatchRange& r) const {
 // cheaper. seg_cost: relative cost of one of its segments.
 bool Engine::batch_range(uint64_t lo, uint64_t hi, uint32_t kinds, BatchRange& r, double& seg_cost) {
   const uint64_t span = (uint64_t) seg_bytes_ * 30u;
-  const uint32_t n_small_all = count_primes_le(small_limit_, true);   // inside the exact head
+  const uint32_t small = batch_params(hi).small_limit ? batch_params(hi).small_limit : small_limit_;
+  const uint32_t n_small_all = count_primes_le(small, true);           // inside the exact head
   const uint64_t seg_low0 = lo - ((lo - 7) % 30 + 7);
   const uint64_t nseg = (hi - 7 - seg_low0) / span + 1;
   const uint32_t n_total = count_primes_upper(isqrt_u64(hi));
@@ -146,8 +147,9 @@ int Engine::batch_class(uint64_t stop) {
 // Autotuner. Range class = decimal digits of stop. For every class present
 // in q: its ranges (all of them up to ~2e12 integers, else a selection by
 // length rank that keeps the longest) are counted once to warm up, then
-// timed under each candidate (direct budget x direct-tier extent); the class
-// keeps the fastest if it beats the defaults by more than 3%. (Small samples
+// timed under each candidate (direct budget x direct-tier extent, then the
+// small/medium threshold halved and doubled from the best of those); the
+// class keeps the fastest if it beats the defaults by more than 3%. (Small samples
 // under-fill the persistent grid and mislead the choice.)
 // Candidates are tried in order until budget_s is used up; the defaults
 // stay where nothing was timed.
@@ -164,6 +166,7 @@ int Engine::autotune_batch(const RangeQuery* q, size_t n, double budget_s, std::
   const uint32_t big_candidates[2] = { big_limit_, (uint32_t) std::min<uint64_t>(span / 4, 0xffffffffull) };
   const double budgets[3] = { 1e7, 1e8, 1e9 };
   const uint32_t stripes[1] = { 8 };
+  const uint32_t small_candidates[2] = { small_limit_ / 2, small_limit_ * 2 };
   std::vector<uint64_t> rows;
   int rc = PSG_OK;
   for (int c = 0; c < kBatchClasses && elapsed() < budget_s; c++) {
@@ -192,23 +195,42 @@ int Engine::autotune_batch(const RangeQuery* q, size_t n, double budget_s, std::
     rep.default_seconds = 0;
     BatchClassParams best = keep;
     bool first = true;
+    bool over = false;
+    const auto time_candidate = [&](const BatchClassParams& cand, double& sec) -> int {
+      batch_tune_[c] = cand;
+      int r = PSG_OK;
+      if (first && (r = count_batch(sample.data(), sample.size(), rows.data(), err))) return r;   // warm-up
+      first = false;
+      const Clock::time_point t0 = Clock::now();
+      if ((r = count_batch(sample.data(), sample.size(), rows.data(), err))) return r;
+      sec = std::chrono::duration<double>(Clock::now() - t0).count();
+      return PSG_OK;
+    };
+    // stage 1: batch-kernel budget x direct-tier extent of bucket-path ranges
     for (double db : budgets)
       for (uint32_t bl : big_candidates)
         for (uint32_t st : stripes) {
-          if (!first && elapsed() > budget_s) break;
+          if (!first && elapsed() > budget_s) { over = true; break; }
           BatchClassParams cand;
           cand.direct_budget = db;
           cand.big_limit = bl;
           cand.stripe = st;
-          batch_tune_[c] = cand;
-          if (first && (rc = count_batch(sample.data(), sample.size(), rows.data(), err))) return rc;   // warm-up
-          first = false;
-          const Clock::time_point t0 = Clock::now();
-          if ((rc = count_batch(sample.data(), sample.size(), rows.data(), err))) return rc;
-          const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
+          double sec = 0;
+          if ((rc = time_candidate(cand, sec))) return rc;
           if (db == 1e8 && bl == big_limit_ && st == 8) rep.default_seconds = sec;
           if (sec < rep.best_seconds) { rep.best_seconds = sec; best = cand; }
         }
+    // stage 2, from the best of stage 1: the small/medium threshold (the
+    // primes below it are crossed off warp-cooperatively, the rest by the
+    // carried wheel walk)
+    for (uint32_t sl : small_candidates) {
+      if (over || elapsed() > budget_s) break;
+      BatchClassParams cand = best;
+      cand.small_limit = sl;
+      double sec = 0;
+      if ((rc = time_candidate(cand, sec))) return rc;
+      if (sec < rep.best_seconds) { rep.best_seconds = sec; best = cand; }
+    }
     // keep the defaults unless a candidate wins clearly (timing noise)
     if (rep.default_seconds > 0 && rep.best_seconds > (1.0 - kTuneMargin) * rep.default_seconds) {
       best = keep;
@@ -304,7 +326,7 @@ int Engine::count_batch(const RangeQuery* q, size_t n, uint64_t* out, std::strin
   for (size_t j = 0; j < bucket_ranges.size(); j++) {
     const size_t i = bucket_ranges[j];
     RangePlan p;
-    rc = plan_range(lo[i], hi[i], p, err, batch_params(hi[i]).big_limit);
+    rc = plan_range(lo[i], hi[i], p, err, batch_params(hi[i]).big_limit, batch_params(hi[i]).small_limit);
     if (rc) return rc;
     rc = run_windows(p, kinds[i], d_batch_rows_ + 6 * (br.size() + j), stream_, 0, p.windows(), err);
     if (rc) return rc;

@@ -368,6 +368,8 @@ int psg_autotune_batch(psg_context* ctx, const psg_range* ranges, size_t n, doub
       o.direct_budget = rep[i].chosen.direct_budget;
       o.big_limit = rep[i].chosen.big_limit;
       o.stripe = rep[i].chosen.stripe;
+      o.small_limit = rep[i].chosen.small_limit;
+      o.reserved = 0;
       o.best_seconds = rep[i].best_seconds;
       o.default_seconds = rep[i].default_seconds;
     }

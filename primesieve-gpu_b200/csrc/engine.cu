@@ -867,7 +867,8 @@ void Engine::fill_common_args(SieveArgs& a) const {
 }
 
 // Prime tiers and launch geometry of [lo, hi] (lo >= 7, lo <= hi).
-int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit) {
+int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit,
+                       uint32_t small_limit) {
   const uint32_t big = big_limit ? big_limit : big_limit_;
   const uint64_t span = (uint64_t) seg_bytes_ * 30u;
   p.lo = lo;
@@ -881,7 +882,7 @@ int Engine::plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err,
   const auto upto = [&](uint64_t v) { return count_primes_le(v, false); };
   const auto below = [&](uint64_t v) { return count_primes_le(v, true); };
   p.n_total = upto(sq);
-  p.n_small = std::min(below(small_limit_), p.n_total);
+  p.n_small = std::min(below(small_limit ? small_limit : small_limit_), p.n_total);
   // medium primes must fit the shared-memory state area
   p.n_med = std::max(p.n_small, std::min({ below(big), p.n_total, p.n_small + state_cap_ }));
   // beyond the shared state and below big: direct tier (no state);

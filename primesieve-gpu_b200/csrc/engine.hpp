@@ -50,6 +50,7 @@ struct BatchClassParams {
   double direct_budget = 1e8;   // segments x primes past the shared state: batch kernel up to this
   uint32_t big_limit = 0;       // bucket-path ranges: direct tier below this prime (0: engine default)
   uint32_t stripe = 8;          // segments per batch-kernel work item
+  uint32_t small_limit = 0;     // warp-cooperative tier below this prime (0: engine default)
 };
 constexpr int kBatchClasses = 21;   // stop < 10^20
 
@@ -123,7 +124,8 @@ public:
   // the alternation continues from one call to the next, so that windows
   // of consecutive ranges overlap too (the caller orders everything the
   // ranges share before chain_begin and reads results after chain_end).
-  int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit = 0);
+  int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit = 0,
+                 uint32_t small_limit = 0);
   int run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
                   cudaStream_t st, uint64_t w0, uint64_t nw, std::string& err);
   void chain_begin(cudaStream_t st);

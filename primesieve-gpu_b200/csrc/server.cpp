@@ -292,7 +292,8 @@ int Server::step(std::vector<Request*>& admitted, std::string& err) {
       std::lock_guard<std::mutex> lk(mu_);
       stats_.batch_requests++;
     } else {
-      int rc = eng_.plan_range(lo, hi, r->plan, err, eng_.batch_params(hi).big_limit);
+      int rc = eng_.plan_range(lo, hi, r->plan, err, eng_.batch_params(hi).big_limit,
+                               eng_.batch_params(hi).small_limit);
       if (rc == PSG_OK && eng_.bucket_bytes(r->plan) > hbm_budget_) {
         rc = PSG_ERR_NOMEM;
         err = "bucket storage of [" + std::to_string(r->start) + ", " + std::to_string(r->stop) +
