@@ -42,6 +42,7 @@ struct BucketArgs {
   const uint64_t* recip;
   const uint32_t* chunk_begin;  // [CTAs + 1] group-walk prime range per CTA
   const uint32_t* thread_chunk; // [CTAs + 1] thread-walk prime range per CTA
+  const uint32_t* far_chunk;    // [CTAs + 1] range of primes above twice the window per CTA
   uint32_t num_lists;         // lists per segment, all kernels
   const uint32_t* list_off;   // [num_lists] entry offset inside a segment region
   const uint32_t* list_cap;   // [num_lists] capacity
@@ -151,6 +152,10 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   const uint32_t hi = a.chunk_begin[blockIdx.x + 1];
   const uint32_t t_lo = a.thread_chunk[blockIdx.x];
   const uint32_t t_hi = a.thread_chunk[blockIdx.x + 1];
+  const uint32_t f_lo = a.far_chunk[blockIdx.x];
+  const uint32_t f_hi = a.far_chunk[blockIdx.x + 1];
+  uint32_t rr = 0;                                // round slot (block-uniform)
+  uint32_t in_bins = 0;                           // entries since the last flush (block-uniform)
   const uint32_t steps = a.tile_steps;
   constexpr uint32_t kFull = 0xffffffffu;
   constexpr uint32_t kDone = 0xffffffffu;
@@ -287,7 +292,7 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
         }
       }
       const int more = __syncthreads_or(warp_done ? 0 : 1);
-      flush(!more && t_lo >= t_hi);     // the CTA's final flush writes the partial quads
+      flush(!more && t_lo >= t_hi && f_lo >= f_hi);   // the CTA's final flush writes the partial quads
       if (!more) break;
     }
   }
@@ -298,8 +303,6 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   if (t_lo < t_hi) {
     const uint32_t nchunk = (t_hi - t_lo + kChunk - 1) / kChunk;
     const uint32_t flush_at = a.flush_at;
-    uint32_t rr = 0;                              // round slot (block-uniform)
-    uint32_t in_bins = 0;                         // entries since the last flush (block-uniform)
     const float tstagger = (float) tid / (float) BLOCK;
     auto issue = [&](uint32_t k) {
       const uint32_t i = t_lo + k * kChunk + tid;
@@ -389,13 +392,79 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
         const int more = __syncthreads_or(tb < tend ? 1 : 0);
         in_bins += s_round[rr];
         rr = rr == 2 ? 0 : rr + 1;
-        const bool last = !more && k + 1 == nchunk;
+        const bool last = !more && k + 1 == nchunk && f_lo >= f_hi;
         if (in_bins >= flush_at || last) {
           flush(last);                            // ends with a barrier
           in_bins = 0;
         }
         if (!more) break;
         emitted = 0;
+      }
+    }
+  }
+
+  // ---- phase 3: primes above twice the window, [f_lo, f_hi): at most four
+  // multiples each in the window, so the per-prime staging and the round
+  // bookkeeping of phase 2 would cost more than the walk. Each thread takes
+  // kFU primes per step, loaded straight from global memory (coalesced, the
+  // next step's loads in flight while this step walks) and walks each at
+  // once; the CTA checks the bins once per step.
+  if (f_lo < f_hi) {
+    constexpr uint32_t kFU = 4;
+    uint32_t pn[kFU];
+    uint64_t rn[kFU];
+    auto load = [&](uint32_t base) {
+#pragma unroll
+      for (uint32_t u = 0; u < kFU; u++) {
+        const uint32_t i = base + u * BLOCK + tid;
+        pn[u] = i < f_hi ? __ldg(a.primes + i) : 0u;
+        rn[u] = i < f_hi ? __ldg(a.recip + i) : 0ull;
+      }
+    };
+    load(f_lo);
+    for (uint32_t base = f_lo; base < f_hi; base += kFU * BLOCK) {
+      uint32_t pc[kFU];
+      uint64_t rc[kFU];
+#pragma unroll
+      for (uint32_t u = 0; u < kFU; u++) { pc[u] = pn[u]; rc[u] = rn[u]; }
+      if (base + kFU * BLOCK < f_hi) load(base + kFU * BLOCK);
+      uint32_t emitted = 0;
+#pragma unroll
+      for (uint32_t u = 0; u < kFU; u++) {          // unrolled: pc and rc stay in registers
+        const uint32_t p = pc[u];
+        if (p == 0) continue;
+        uint64_t d; uint32_t c0;
+        first_multiple(a.win_low, p, rc[u], d, c0);
+        uint32_t j = first_class_ge(c0);
+        const uint64_t b64 = (d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u;
+        if (b64 >= win_bytes) continue;
+        uint32_t tb = (uint32_t) b64;
+        const uint32_t tpd = p / 30u;
+        const uint32_t cls = residue_to_bit(p - 30u * tpd);
+        const uint32_t tbits = wheel_tab[2 * cls];
+        const uint32_t tcorr = wheel_tab[2 * cls + 1];
+        do {
+          uint32_t bo;
+          const uint32_t sg = split_b(tb, bo);
+          const uint32_t sh = 3u * j;
+          put(sg, atomicAdd(&cnt[sg], 1u), (bo << 3) | ((tbits >> sh) & 7u));
+          emitted++;
+          // tb < 2^31 and the step < 2^30: no wrap
+          tb += tpd * ((kGapPacked >> sh) & 7u) + ((tcorr >> sh) & 7u);
+          j = (j + 1u) & 7u;
+        } while (tb < win_bytes);
+      }
+      // the round protocol of phase 2 (three rotating count slots, one barrier)
+      emitted = __reduce_add_sync(kFull, emitted);
+      if (lane == 0 && emitted) atomicAdd(&s_round[rr], emitted);
+      if (tid == 0) s_round[rr == 2 ? 0 : rr + 1] = 0;
+      __syncthreads();
+      in_bins += s_round[rr];
+      rr = rr == 2 ? 0 : rr + 1;
+      const bool last = base + kFU * BLOCK >= f_hi;
+      if (in_bins >= a.flush_at || last) {
+        flush(last);                              // ends with a barrier
+        in_bins = 0;
       }
     }
   }

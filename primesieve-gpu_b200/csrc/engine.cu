@@ -37,6 +37,7 @@ namespace {
 constexpr int kBucketBlock = 1024;
 constexpr double kSetupGroup = 8.0;     // fill-chunk cost of locating a group-walk prime (entries)
 constexpr double kSetupThread = 4.0;    // ... of a thread-walk prime
+constexpr double kSetupFar = 2.5;       // ... of a prime above twice the window (four per thread and step)
 // Bucket fill bins: group-walk steps per warp between flushes (as a fill
 // fraction of the bins) and the thread walk's flush threshold; group-walk
 // primes with at least kStaggerMultiples multiples per class and window
@@ -659,7 +660,9 @@ int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
     // cost over the 1/p prefix table); CTA c takes chunk c of both.
     const double setup_group = kSetupGroup, setup_thread = kSetupThread;
     const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), first), last);
-    begin.assign(2 * (fill_ctas + 1), 0);
+    // primes above twice the window: at most four multiples per window
+    const uint32_t f_end = std::min(std::max(approx_count_below(2ull * window_ * seg_bytes_ + 1), t_end), last);
+    begin.assign(3 * (fill_ctas + 1), 0);
     const auto cut = [&](uint32_t from, uint32_t to, double setup, uint32_t* bounds) {
       const double s0 = inv_prefix(from);
       const auto cost = [&](uint32_t i) { return setup * (double) (i - from) + win_span * (inv_prefix(i) - s0); };
@@ -678,11 +681,14 @@ int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
     };
     cut(first, t_end, setup_group, begin.data());
     uint32_t* tchunk = begin.data() + fill_ctas + 1;
-    cut(t_end, last, setup_thread, tchunk);
+    cut(t_end, f_end, setup_thread, tchunk);
+    uint32_t* fchunk = tchunk + fill_ctas + 1;
+    cut(f_end, last, kSetupFar, fchunk);
     std::vector<double> mu(fill_ctas, 0.0);
     for (uint32_t c = 0; c < fill_ctas; c++)
       mu[c] = per_seg * (inv_prefix(begin[c + 1]) - inv_prefix(begin[c]) +
-                         inv_prefix(tchunk[c + 1]) - inv_prefix(tchunk[c]));
+                         inv_prefix(tchunk[c + 1]) - inv_prefix(tchunk[c]) +
+                         inv_prefix(fchunk[c + 1]) - inv_prefix(fchunk[c]));
     for (uint32_t c = 0; c < fill_ctas; c++) add_list(mu[c]);
   }
   const uint32_t lists = fill_ctas;
@@ -725,7 +731,7 @@ int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
   }
   plan_.table.assign(off.begin(), off.end());
   plan_.table.insert(plan_.table.end(), cap.begin(), cap.end());
-  if (fill_ctas) plan_.table.insert(plan_.table.end(), begin.begin(), begin.begin() + 2 * (fill_ctas + 1));
+  if (fill_ctas) plan_.table.insert(plan_.table.end(), begin.begin(), begin.begin() + 3 * (fill_ctas + 1));
   plan_.first = first;
   plan_.last = last;
   plan_.geom.seg_stride = stride;
@@ -746,7 +752,7 @@ int Engine::plan_to_slot(uint32_t set, cudaStream_t ws, std::string& err) {
   const size_t n = plan_.table.size();
   // sized once for any plan of lists_ fill lists: growing
   // waits for every window in flight
-  const size_t want = std::max<size_t>(n, 4 * (size_t) lists_ + 8);
+  const size_t want = std::max<size_t>(n, 5 * (size_t) lists_ + 8);
   if (n > sl.cap) {
     if (sl.d_table) quiesce();        // the old table may still be read
     cudaFree(sl.d_table); sl.d_table = nullptr; sl.cap = 0;
@@ -979,6 +985,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         b.recip = d_recip_;
         b.chunk_begin = t_chunk;
         b.thread_chunk = t_chunk + gm.fill_ctas + 1;
+        b.far_chunk = t_chunk + 2 * (gm.fill_ctas + 1);
         b.num_lists = gm.lists;
         b.list_off = t_off;
         b.list_cap = t_cap;
