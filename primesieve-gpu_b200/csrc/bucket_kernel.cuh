@@ -42,7 +42,7 @@ struct BucketArgs {
   const uint64_t* recip;
   const uint32_t* chunk_begin;  // [CTAs + 1] group-walk prime range per CTA
   const uint32_t* thread_chunk; // [CTAs + 1] thread-walk prime range per CTA
-  const uint32_t* far_chunk;    // [CTAs + 1] range of primes above twice the window per CTA
+  const uint32_t* far_chunk;    // [CTAs + 1] range of primes above the window per CTA
   uint32_t num_lists;         // lists per segment, all kernels
   const uint32_t* list_off;   // [num_lists] entry offset inside a segment region
   const uint32_t* list_cap;   // [num_lists] capacity
@@ -403,12 +403,13 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
     }
   }
 
-  // ---- phase 3: primes above twice the window, [f_lo, f_hi): at most four
-  // multiples each in the window, so the per-prime staging and the round
-  // bookkeeping of phase 2 would cost more than the walk. Each thread takes
-  // kFU primes per step, loaded straight from global memory (coalesced, the
-  // next step's loads in flight while this step walks) and walks each at
-  // once; the CTA checks the bins once per step.
+  // ---- phase 3: primes above the window's byte length, [f_lo, f_hi): at
+  // most eight multiples each in the window, so the per-prime staging and
+  // the round bookkeeping of phase 2 would cost more than the walk. Each
+  // thread takes kFU primes per step, loaded straight from global memory
+  // (coalesced, the next step's loads in flight while this step walks) and
+  // walks each at once; the CTA checks the bins once per step. (Eight primes
+  // per step measured slower: register spills.)
   if (f_lo < f_hi) {
     constexpr uint32_t kFU = 4;
     uint32_t pn[kFU];

@@ -37,7 +37,7 @@ namespace {
 constexpr int kBucketBlock = 1024;
 constexpr double kSetupGroup = 8.0;     // fill-chunk cost of locating a group-walk prime (entries)
 constexpr double kSetupThread = 4.0;    // ... of a thread-walk prime
-constexpr double kSetupFar = 2.5;       // ... of a prime above twice the window (four per thread and step)
+constexpr double kSetupFar = 2.5;       // ... of a prime above the window (four per thread and step)
 // Bucket fill bins: group-walk steps per warp between flushes (as a fill
 // fraction of the bins) and the thread walk's flush threshold; group-walk
 // primes with at least kStaggerMultiples multiples per class and window
@@ -660,8 +660,10 @@ int Engine::ensure_buckets(uint32_t first, uint32_t last, std::string& err) {
     // cost over the 1/p prefix table); CTA c takes chunk c of both.
     const double setup_group = kSetupGroup, setup_thread = kSetupThread;
     const uint32_t t_end = std::min(std::max(approx_count_below(thread_limit(window_)), first), last);
-    // primes above twice the window: at most four multiples per window
-    const uint32_t f_end = std::min(std::max(approx_count_below(2ull * window_ * seg_bytes_ + 1), t_end), last);
+    // primes above the window's byte length: at most eight multiples per
+    // window (the threshold twice as high measured 1-2% slower at 1e18 and
+    // near 2^64)
+    const uint32_t f_end = std::min(std::max(approx_count_below(1ull * window_ * seg_bytes_ + 1), t_end), last);
     begin.assign(3 * (fill_ctas + 1), 0);
     const auto cut = [&](uint32_t from, uint32_t to, double setup, uint32_t* bounds) {
       const double s0 = inv_prefix(from);

@@ -271,8 +271,8 @@ private:
   cudaEvent_t fork_event_ = nullptr, join_event_ = nullptr;
   // Bucket plan of the current big primes [first, last) (host): geometry and
   // one u32 table [lists offsets | lists capacities | 3 (fill_ctas + 1)
-  // fill chunk bounds: group walk, thread walk, primes above twice the
-  // window]; gen changes with every new plan.
+  // fill chunk bounds: group walk, thread walk, primes above the window];
+  // gen changes with every new plan.
   struct PlanGeom {
     uint64_t seg_stride = 0;              // entries per segment region
     uint32_t lists = 0, fill_ctas = 0;
