@@ -30,6 +30,7 @@ namespace psg {
 
 struct BucketArgs {
   uint64_t win_low;           // segLow of the window's first segment
+  uint32_t sqrt_x0;           // floor(sqrt(win_low + 6)): p <= sqrt_x0 <=> p*p < win_low + 7
   uint32_t win_segments;      // segments in this window (<= counters in smem)
   uint32_t seg_bytes;
   uint32_t seg_magic;         // floor(2^32 / seg_bytes) + 1 (segment index)
@@ -412,6 +413,7 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
   // per step measured slower: register spills.)
   if (f_lo < f_hi) {
     constexpr uint32_t kFU = 4;
+    const uint64_t x0 = a.win_low + 7u;
     uint32_t pn[kFU];
     uint64_t rn[kFU];
     auto load = [&](uint32_t base) {
@@ -434,14 +436,35 @@ bucket_fill_kernel(const __grid_constant__ BucketArgs a)
       for (uint32_t u = 0; u < kFU; u++) {          // unrolled: pc and rc stay in registers
         const uint32_t p = pc[u];
         if (p == 0) continue;
-        uint64_t d; uint32_t c0;
-        first_multiple(a.win_low, p, rc[u], d, c0);
-        uint32_t j = first_class_ge(c0);
-        const uint64_t b64 = (d + (uint64_t) (cofactor_class(j) - c0) * p) / 30u;
-        if (b64 >= win_bytes) continue;
-        uint32_t tb = (uint32_t) b64;
+        // the first multiple's offset d from x0 as 30 * dq + dm and its
+        // cofactor's residue c0 (first_multiple's cases, the p*p test by the
+        // window's square root); then with p = 30 * tpd + pm and k the gap to
+        // the first wheel class, byte = (d + k * p) / 30
+        //   = dq + k * tpd + (dm + k * pm) / 30, all in 32 bits
         const uint32_t tpd = p / 30u;
-        const uint32_t cls = residue_to_bit(p - 30u * tpd);
+        const uint32_t pm = p - 30u * tpd;
+        uint32_t dq, dm, c0;
+        if (p <= a.sqrt_x0) {
+          const uint32_t r = mod_recip(x0, p, rc[u]);
+          const uint32_t dd = r ? p - r : 0u;
+          dq = dd / 30u;                          // < 2^28
+          dm = dd - 30u * dq;
+          const uint32_t t = dm < 23u ? dm + 7u : dm - 23u;   // (7 + d) mod 30
+          c0 = (t * inverse_mod30(pm)) % 30u;
+        } else {
+          const uint64_t d = (uint64_t) p * p - x0;
+          if (d >= 30ull * win_bytes) continue;   // p*p beyond the window
+          dq = (uint32_t) (d / 30u);              // < win_bytes
+          dm = (uint32_t) d - 30u * dq;
+          c0 = pm;
+        }
+        uint32_t j = first_class_ge(c0);
+        const uint32_t k = cofactor_class(j) - c0;   // < 30
+        const uint32_t kt = k * tpd;                  // < p < 2^32
+        if (kt >= win_bytes) continue;
+        uint32_t tb = kt + dq + (dm + k * pm) / 30u;  // < 2^31 + 2^28 + 30
+        if (tb >= win_bytes) continue;
+        const uint32_t cls = residue_to_bit(pm);
         const uint32_t tbits = wheel_tab[2 * cls];
         const uint32_t tcorr = wheel_tab[2 * cls + 1];
         do {

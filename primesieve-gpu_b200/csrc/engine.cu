@@ -968,6 +968,7 @@ int Engine::run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* 
         BucketArgs b;
         std::memset(&b, 0, sizeof b);
         b.win_low = win_low;
+        b.sqrt_x0 = isqrt_u64(win_low + 6u);
         b.win_segments = (uint32_t) ns;
         b.seg_bytes = seg_bytes_;
         b.seg_magic = (uint32_t) ((1ull << 32) / seg_bytes_ + 1u);

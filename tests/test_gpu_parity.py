@@ -120,6 +120,28 @@ def test_additivity_full_size(ctx, ref_counts, psg):
     assert total == row["counts"]
 
 
+def test_random_chunks_sum(psg):
+    """The reference's chunked-count test (test/count_primes3.cpp:31-57):
+    [1e12, 1e12+1e9] cut into seeded random chunks (any cut, not only at
+    == 2 (mod 30), so primes only), each counted by a context with a
+    different segment size and bucket window, sums to 36190991."""
+    rng = random.Random(1234)
+    a, b = 10 ** 12, 10 ** 12 + 10 ** 9
+    cuts = sorted(rng.sample(range(a + 1, b), 40))
+    bounds = [a] + cuts + [b + 1]
+    configs = [dict(), dict(seg_bytes=16384, block=512, window_segments=7),
+               dict(seg_bytes=65536, block=1024, big_limit=100000, window_segments=3)]
+    ctxs = [psg.Context(**c) for c in configs]
+    try:
+        total = 0
+        for i, (x, y) in enumerate(zip(bounds, bounds[1:])):
+            total += ctxs[i % len(ctxs)].count(x, y - 1, 1)[0]
+    finally:
+        for c in ctxs:
+            c.close()
+    assert total == 36190991
+
+
 def test_empty_and_single(ctx):
     assert ctx.count(10, 5) == [0] * 6
     assert ctx.count(0, 0) == [0] * 6
