@@ -49,11 +49,13 @@ METRIC = "integers sieved/s, exact pi/k-tuplet counts: batched vs per-range; p50
 UNIT = "integers/s"
 WORKLOAD = "count primes in [1e15, 1e15+1e11] (sieving primes <= 3.16e7, bucket sieve)"
 GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
-# ncu, [1e15, 1e15+2e9] (one window, 167,958,746 bucket entries):
-# fill kernel 612.604416 MB written + 67.080192 MB read, sieve kernel
-# 667.471872 MB read + 6.376192 MB written
-FILL_DRAM_BYTES_PER_ENTRY = (612.604416e6 + 67.080192e6) / 167958746
-SIEVE_DRAM_BYTES_PER_ENTRY = (667.471872e6 + 6.376192e6) / 167958746
+# ncu, [1e15, 1e15+4e9] (one 1018-segment window of the default engine,
+# 312,728,441 bucket entries: the multiples of the primes 393,216..3.16e7
+# with cofactors prime to 30, counted exactly on the host): fill kernel
+# 1335.764 MB written + 171.315 MB read, sieve kernel 1358.760 MB read +
+# 6.641 MB written
+FILL_DRAM_BYTES_PER_ENTRY = (1335.764e6 + 171.314688e6) / 312728441
+SIEVE_DRAM_BYTES_PER_ENTRY = (1358.760e6 + 6.640640e6) / 312728441
 
 
 CONFIGS = [
@@ -345,7 +347,7 @@ def main():
     sieve_rate = crossings / max(sieve_ms * 1e-3, 1e-12)
     dominant = "bucket_fill_kernel" if fill_ms > sieve_ms else "sieve_count_kernel"
     # DRAM traffic per launch: bytes per bucket entry from one ncu capture of
-    # each kernel on [1e15, 1e15+2e9] (one 509-segment window, 167,958,746
+    # each kernel on [1e15, 1e15+4e9] (one 1018-segment window, 312,728,441
     # entries), scaled by this launch's entries
     entries_per_launch = entries_per_pass / max(fill_l, 1)
     fill_traffic = FILL_DRAM_BYTES_PER_ENTRY * entries_per_launch
