@@ -78,7 +78,8 @@ typedef struct {
   uint32_t seg_bytes;          /* shared-memory sieve segment per CTA (bytes) */
   uint32_t block;              /* threads per CTA: 256, 512 or 1024 */
   uint32_t ctas_per_sm;        /* resident sieve CTAs per SM */
-  uint32_t small_limit;        /* sieving primes below: one warp per prime */
+  uint32_t small_limit;        /* sieving primes below: one warp per prime (0: per range,
+                                  4096, 2048 or 1024 as sqrt(stop) grows past 2e6 and 8e6) */
   uint32_t big_limit;          /* sieving primes from: bucket sieve */
   uint32_t window_segments;    /* segments per bucket window */
   uint32_t bucket_lists;       /* bucket lists per segment */

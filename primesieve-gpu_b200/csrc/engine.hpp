@@ -124,6 +124,9 @@ public:
   // the alternation continues from one call to the next, so that windows
   // of consecutive ranges overlap too (the caller orders everything the
   // ranges share before chain_begin and reads results after chain_end).
+  // The range kernel's warp-cooperative tier for a range ending at hi: the
+  // config's small_limit, else by the bucket primes' share of the work.
+  uint32_t range_small_limit(uint64_t hi) const;
   int plan_range(uint64_t lo, uint64_t hi, RangePlan& p, std::string& err, uint32_t big_limit = 0,
                  uint32_t small_limit = 0);
   int run_windows(const RangePlan& p, uint32_t kinds, unsigned long long* dev_counts,
@@ -234,6 +237,7 @@ private:
   EngineConfig cfg_;
   uint32_t seg_bytes_ = 0, block_ = 0, grid_ = 0, bucket_block_ = 256;
   uint32_t small_limit_ = 0, big_limit_ = 0, window_ = 0, lists_ = 0;
+  bool small_auto_ = true;        // small_limit_ not set by the config: chosen per range
   uint32_t state_cap_ = 0, smem_dyn_ = 0, seg_shift_ = 0;
   bool seg_pow2_ = true;
 
