@@ -97,6 +97,24 @@ def test_engine_configs(psg, oracle, ref_counts, cfg):
         c.close()
 
 
+def test_small_limit_per_range(psg, oracle, ctx):
+    """By default the warp-cooperative tier ends at 4096, 2048 or 1024 as
+    sqrt(stop) passes 2e6 and 8e6; ranges on both sides of each switch
+    count the same as the oracle and as contexts with each limit fixed."""
+    ranges = [(4 * 10 ** 12 - 10 ** 7, 4 * 10 ** 12 - 1), (4 * 10 ** 12, 4 * 10 ** 12 + 10 ** 7),
+              (64 * 10 ** 12 - 10 ** 7, 64 * 10 ** 12 - 1), (64 * 10 ** 12, 64 * 10 ** 12 + 10 ** 7)]
+    fixed = [psg.Context(small_limit=s) for s in (4096, 2048, 1024)]
+    try:
+        for a, b in ranges:
+            want = oracle.plain(a, b)
+            assert ctx.count(a, b) == want, (a, b)
+            for c in fixed:
+                assert c.count(a, b) == want, (a, b)
+    finally:
+        for c in fixed:
+            c.close()
+
+
 def test_contexts_with_different_layouts_coexist(psg, ctx):
     """Kernel shared-memory limits are per process, not per context: a
     context with small segments and windows, created and used after the
