@@ -52,10 +52,10 @@ GOLDEN_1E15 = 2895317534          # pi[1e15, 1e15+1e11], reference CPU library
 # ncu, [1e15, 1e15+4e9] (one 1018-segment window of the default engine,
 # 312,728,441 bucket entries: the multiples of the primes 393,216..3.16e7
 # with cofactors prime to 30, counted exactly on the host): fill kernel
-# 1335.764 MB written + 171.315 MB read, sieve kernel 1358.760 MB read +
-# 6.641 MB written
-FILL_DRAM_BYTES_PER_ENTRY = (1335.764e6 + 171.314688e6) / 312728441
-SIEVE_DRAM_BYTES_PER_ENTRY = (1358.760e6 + 6.640640e6) / 312728441
+# 1332.425 MB written + 166.158 MB read, sieve kernel 1358.508 MB read +
+# 5.942 MB written
+FILL_DRAM_BYTES_PER_ENTRY = (1332.425e6 + 166.157824e6) / 312728441
+SIEVE_DRAM_BYTES_PER_ENTRY = (1358.508e6 + 5.942016e6) / 312728441
 
 
 CONFIGS = [
